@@ -1,0 +1,130 @@
+/*
+ * pirate_b200.h -- C ABI of the B200 real-time dedispersion path.
+ *
+ * This is the drop-in boundary for pirate's dedispersion hot path: tree gridding, lagged
+ * downsampling, two-stage tree dedispersion, lag staging and peak finding on one GPU. Each entry
+ * point names the pirate interface it replaces (file:line in the pirate source tree).
+ *
+ * Conventions: every function returns 0 on success and a nonzero status on error; the message of the
+ * most recent error on the calling thread is returned by pb2_last_error(). Handles are opaque.
+ * CUDA streams are passed as `void *` (a cudaStream_t; NULL is the legacy default stream).
+ * A pb2_dedisperser is thread safe in the same sense as pirate's GpuDedisperser: calls are
+ * serialized internally; seq_id cursors must advance 0, 1, 2, ... per cursor.
+ */
+#ifndef PIRATE_B200_H
+#define PIRATE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB2_MAX_TREES 64
+
+typedef struct pb2_config pb2_config;
+typedef struct pb2_plan pb2_plan;
+typedef struct pb2_dedisperser pb2_dedisperser;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *pb2_last_error(void);
+
+/* Library version string. */
+const char *pb2_version(void);
+
+/* ---- DedispersionConfig (include/pirate/DedispersionConfig.hpp:21-194) ---- */
+
+/* DedispersionConfig::from_yaml(filename), src_lib/DedispersionConfig.cpp:651 */
+int pb2_config_from_yaml(const char *path, pb2_config **out);
+/* DedispersionConfig::from_yaml(YamlFile) on an in-memory document, src_lib/DedispersionConfig.cpp:659 */
+int pb2_config_from_yaml_string(const char *text, pb2_config **out);
+/* DedispersionConfig::to_yaml_string(), src_lib/DedispersionConfig.cpp:638. Writes at most buflen bytes
+ * (NUL-terminated); *needed receives the full length + 1. */
+int pb2_config_to_yaml(const pb2_config *cfg, char *buf, long buflen, long *needed);
+/* DedispersionConfig::make_channel_map(), src_lib/DedispersionConfig.cpp:239; out has 2^rank + 1 doubles. */
+int pb2_config_channel_map(const pb2_config *cfg, double *out, long n);
+/* DedispersionConfig::{delay_to_frequency, frequency_to_delay, dm_per_unit_delay}, src_lib/DedispersionConfig.cpp:135-214 */
+int pb2_config_delay_to_frequency(const pb2_config *cfg, double delay, double *freq);
+int pb2_config_frequency_to_delay(const pb2_config *cfg, double freq, double *delay);
+int pb2_config_dm_per_unit_delay(const pb2_config *cfg, double *dm);
+void pb2_config_destroy(pb2_config *cfg);
+
+/* ---- DedispersionPlan (include/pirate/DedispersionPlan.hpp:33-225) ---- */
+
+typedef struct pb2_tree_info {
+    long primary_tree_index, early_trigger_level, amb_rank, dd_rank, nt_ds;
+    long ndm_out, nt_out, ndm_wt, nt_wt, nprofiles, Dcore;
+    long max_width, dm_downsampling, time_downsampling, wt_dm_downsampling, wt_time_downsampling;
+    long nsubbands /* N */, nmultiplets /* M */, pf_rank;
+    double dm_min, dm_max, trigger_frequency;
+} pb2_tree_info;
+
+/* DedispersionPlan(config), src_lib/DedispersionPlan.cpp:29 */
+int pb2_plan_create(const pb2_config *cfg, pb2_plan **out);
+void pb2_plan_destroy(pb2_plan *plan);
+/* DedispersionPlan::to_yaml_string(), src_lib/DedispersionPlan.cpp:900 (tree section; no MegaRingbuf zones) */
+int pb2_plan_to_yaml(const pb2_plan *plan, char *buf, long buflen, long *needed);
+/* DedispersionPlan::ntrees / trees[i] (include/pirate/DedispersionTree.hpp:19-59) */
+int pb2_plan_ntrees(const pb2_plan *plan, long *ntrees);
+int pb2_plan_tree_info(const pb2_plan *plan, long itree, pb2_tree_info *out);
+/* DedispersionPlan::stage1_dd_rank / stage1_amb_rank (length num_primary_trees) */
+int pb2_plan_stage1_ranks(const pb2_plan *plan, long *dd_rank, long *amb_rank, long n);
+/* DedispersionPlan::decode_argmax, src_lib/DedispersionPlan.cpp:481; out5 = (fmin, fmax, tlo, thi, p) */
+int pb2_plan_decode_argmax(const pb2_plan *plan, uint32_t token, long itree, long idm, long itime, long *out5);
+/* DedispersionPlan::decode_argmax2, src_lib/DedispersionPlan.cpp:544; out5 = (freq_lo, freq_hi, dm, time, width) */
+int pb2_plan_decode_argmax2(const pb2_plan *plan, long itree, const long *in5, double *out5);
+/* DedispersionPlan::compute_steady_state_it0, src_lib/DedispersionPlan.cpp:634; out has ndm_out entries */
+int pb2_plan_steady_state_it0(const pb2_plan *plan, long itree, long *out, long n);
+
+/* ---- GpuDedisperser (include/pirate/Dedisperser.hpp:45-254) ---- */
+
+/* GpuDedisperser::Params, include/pirate/Dedisperser.hpp:47-86 (the stream pool is internal). */
+typedef struct pb2_dd_params {
+    int cuda_device_id;
+    long nbatches_out;      /* 0 -> num_active_batches */
+    long nbatches_wt;       /* 0 -> nbatches_out */
+    long num_consumers;
+    int synchronous;
+    long initial_chunk;
+} pb2_dd_params;
+
+/* GpuDedisperser::Outputs, include/pirate/Dedisperser.hpp:98-125. out_max[i] and out_argmax[i] are
+ * device pointers to (nbeams, ndm_out[i], nt_out[i]) arrays; out_max has the config dtype. */
+typedef struct pb2_outputs {
+    int dtype;              /* 0 float32, 1 float16, 2 bfloat16 */
+    long nbeams, ichunk_zero_based, ichunk_fpga_based, ibeam, ntrees;
+    long ndm_out[PB2_MAX_TREES], nt_out[PB2_MAX_TREES];
+    void *out_max[PB2_MAX_TREES];
+    uint32_t *out_argmax[PB2_MAX_TREES];
+} pb2_outputs;
+
+/* GpuDedisperser::create(params), src_lib/GpuDedisperser.cpp:84 */
+int pb2_dd_create(const pb2_plan *plan, const pb2_dd_params *params, pb2_dedisperser **out);
+/* GpuDedisperser::allocate(gpu_allocator, host_allocator), src_lib/GpuDedisperser.cpp:390 (allocates internally) */
+int pb2_dd_allocate(pb2_dedisperser *dd);
+/* Device bytes held by the dedisperser after allocate(). */
+int pb2_dd_device_bytes(const pb2_dedisperser *dd, long *nbytes);
+/* GpuDedisperser::acquire_input, src_lib/GpuDedisperser.cpp:796; shape3 = (beams_per_batch, nfreq, nt_in) */
+int pb2_dd_acquire_input(pb2_dedisperser *dd, long seq_id, void *stream, void **ptr, long *shape3);
+/* GpuDedisperser::release_input_and_launch_dd_kernels, src_lib/GpuDedisperser.cpp:830 */
+int pb2_dd_release_input(pb2_dedisperser *dd, long seq_id, void *stream);
+/* GpuDedisperser::acquire_output, src_lib/GpuDedisperser.cpp:890 (sync != 0 blocks the host) */
+int pb2_dd_acquire_output(pb2_dedisperser *dd, long consumer_id, long seq_id, void *stream, int sync, pb2_outputs *out);
+/* GpuDedisperser::release_output, src_lib/GpuDedisperser.cpp:945 */
+int pb2_dd_release_output(pb2_dedisperser *dd, long consumer_id, long seq_id, void *stream);
+/* GpuDedisperser::fill_all_weights, src_lib/GpuDedisperser.cpp:1240; host array
+ * (nbatches_wt, beams_per_batch, ndm_wt, nt_wt, nprofiles, N) float32 */
+int pb2_dd_fill_weights(pb2_dedisperser *dd, long itree, const float *host, long nelts);
+/* GpuDedisperser::stop, src_lib/GpuDedisperser.cpp:735 */
+int pb2_dd_stop(pb2_dedisperser *dd);
+/* Kernel launches per (chunk, batch), and algorithmic HBM bytes per (chunk, batch) for the
+ * kernel classes [grid, lds, stage1, stage2, pf]. */
+int pb2_dd_kernels_per_batch(const pb2_dedisperser *dd, long *n);
+int pb2_dd_algorithmic_bytes(const pb2_dedisperser *dd, double *out5);
+void pb2_dd_destroy(pb2_dedisperser *dd);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIRATE_B200_H */

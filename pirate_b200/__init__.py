@@ -1,0 +1,387 @@
+"""pirate_b200: B200-native real-time FRB dedispersion (tree gridding, lagged downsampling,
+two-stage tree dedispersion, lag staging and peak finding), behind pirate's
+DedispersionConfig / DedispersionPlan / GpuDedisperser interface.
+
+The compute path is libpirate_b200.so (hand-written sm_100a kernels behind the C ABI of
+include/pirate_b200.h); this module is a thin ctypes mirror of pirate's pybind11 classes
+(src_pybind11/pirate_pybind11.cpp:128-593, pirate_frb/GpuDedisperser.py:123-197).
+There is no CPU fallback: if the library cannot be loaded, every entry point raises.
+"""
+
+import contextlib
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["DedispersionConfig", "DedispersionPlan", "GpuDedisperser", "Outputs", "lib", "LIB_PATH"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpirate_b200.so")
+MAX_TREES = 64
+
+_lib = None
+
+
+class _TreeInfo(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_long) for k in (
+        "primary_tree_index", "early_trigger_level", "amb_rank", "dd_rank", "nt_ds",
+        "ndm_out", "nt_out", "ndm_wt", "nt_wt", "nprofiles", "Dcore",
+        "max_width", "dm_downsampling", "time_downsampling", "wt_dm_downsampling", "wt_time_downsampling",
+        "nsubbands", "nmultiplets", "pf_rank")] + [
+        ("dm_min", ctypes.c_double), ("dm_max", ctypes.c_double), ("trigger_frequency", ctypes.c_double)]
+
+
+class _DdParams(ctypes.Structure):
+    _fields_ = [("cuda_device_id", ctypes.c_int), ("nbatches_out", ctypes.c_long), ("nbatches_wt", ctypes.c_long),
+                ("num_consumers", ctypes.c_long), ("synchronous", ctypes.c_int), ("initial_chunk", ctypes.c_long)]
+
+
+class _Outputs(ctypes.Structure):
+    _fields_ = [("dtype", ctypes.c_int), ("nbeams", ctypes.c_long), ("ichunk_zero_based", ctypes.c_long),
+                ("ichunk_fpga_based", ctypes.c_long), ("ibeam", ctypes.c_long), ("ntrees", ctypes.c_long),
+                ("ndm_out", ctypes.c_long * MAX_TREES), ("nt_out", ctypes.c_long * MAX_TREES),
+                ("out_max", ctypes.c_void_p * MAX_TREES), ("out_argmax", ctypes.c_void_p * MAX_TREES)]
+
+
+def lib():
+    """Loads libpirate_b200.so (built in-tree by pirate_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("pirate_b200: %s is missing; build it with 'python -m pirate_b200.build'" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    vp, lp, cp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.c_char_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "pb2_last_error": (cp, []),
+        "pb2_version": (cp, []),
+        "pb2_config_from_yaml": (ctypes.c_int, [cp, ctypes.POINTER(vp)]),
+        "pb2_config_from_yaml_string": (ctypes.c_int, [cp, ctypes.POINTER(vp)]),
+        "pb2_config_to_yaml": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_long, lp]),
+        "pb2_config_channel_map": (ctypes.c_int, [vp, dp, ctypes.c_long]),
+        "pb2_config_delay_to_frequency": (ctypes.c_int, [vp, ctypes.c_double, dp]),
+        "pb2_config_frequency_to_delay": (ctypes.c_int, [vp, ctypes.c_double, dp]),
+        "pb2_config_dm_per_unit_delay": (ctypes.c_int, [vp, dp]),
+        "pb2_config_destroy": (None, [vp]),
+        "pb2_plan_create": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
+        "pb2_plan_destroy": (None, [vp]),
+        "pb2_plan_to_yaml": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_long, lp]),
+        "pb2_plan_ntrees": (ctypes.c_int, [vp, lp]),
+        "pb2_plan_tree_info": (ctypes.c_int, [vp, ctypes.c_long, ctypes.POINTER(_TreeInfo)]),
+        "pb2_plan_stage1_ranks": (ctypes.c_int, [vp, lp, lp, ctypes.c_long]),
+        "pb2_plan_decode_argmax": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_long, ctypes.c_long, ctypes.c_long, lp]),
+        "pb2_plan_decode_argmax2": (ctypes.c_int, [vp, ctypes.c_long, lp, dp]),
+        "pb2_plan_steady_state_it0": (ctypes.c_int, [vp, ctypes.c_long, lp, ctypes.c_long]),
+        "pb2_dd_create": (ctypes.c_int, [vp, ctypes.POINTER(_DdParams), ctypes.POINTER(vp)]),
+        "pb2_dd_allocate": (ctypes.c_int, [vp]),
+        "pb2_dd_device_bytes": (ctypes.c_int, [vp, lp]),
+        "pb2_dd_acquire_input": (ctypes.c_int, [vp, ctypes.c_long, vp, ctypes.POINTER(vp), lp]),
+        "pb2_dd_release_input": (ctypes.c_int, [vp, ctypes.c_long, vp]),
+        "pb2_dd_acquire_output": (ctypes.c_int, [vp, ctypes.c_long, ctypes.c_long, vp, ctypes.c_int, ctypes.POINTER(_Outputs)]),
+        "pb2_dd_release_output": (ctypes.c_int, [vp, ctypes.c_long, ctypes.c_long, vp]),
+        "pb2_dd_fill_weights": (ctypes.c_int, [vp, ctypes.c_long, vp, ctypes.c_long]),
+        "pb2_dd_stop": (ctypes.c_int, [vp]),
+        "pb2_dd_kernels_per_batch": (ctypes.c_int, [vp, lp]),
+        "pb2_dd_algorithmic_bytes": (ctypes.c_int, [vp, dp]),
+        "pb2_dd_destroy": (None, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError(lib().pb2_last_error().decode())
+
+
+def _yaml_out(fn, handle):
+    n = ctypes.c_long(0)
+    _check(fn(handle, None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value)
+    _check(fn(handle, buf, n.value, ctypes.byref(n)))
+    return buf.value.decode()
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream   # torch.cuda.Stream
+
+
+class DedispersionConfig:
+    """pirate's DedispersionConfig (include/pirate/DedispersionConfig.hpp:21-194): same YAML keys."""
+
+    def __init__(self, handle):
+        self._h = handle
+        import yaml
+        self._d = yaml.safe_load(self.to_yaml_string())
+
+    @staticmethod
+    def from_yaml(path):
+        h = ctypes.c_void_p()
+        _check(lib().pb2_config_from_yaml(os.fsencode(path), ctypes.byref(h)))
+        return DedispersionConfig(h)
+
+    @staticmethod
+    def from_yaml_string(text):
+        h = ctypes.c_void_p()
+        _check(lib().pb2_config_from_yaml_string(text.encode(), ctypes.byref(h)))
+        return DedispersionConfig(h)
+
+    @staticmethod
+    def from_dict(d):
+        import yaml
+        return DedispersionConfig.from_yaml_string(yaml.safe_dump(d, default_flow_style=None, width=1 << 30))
+
+    def to_yaml_string(self):
+        return _yaml_out(lib().pb2_config_to_yaml, self._h)
+
+    def to_dict(self):
+        return dict(self._d)
+
+    def __getattr__(self, k):
+        d = self.__dict__.get("_d")
+        if d is not None and k in d:
+            return d[k]
+        raise AttributeError(k)
+
+    def get_total_nfreq(self):
+        return int(sum(self._d["zone_nfreq"]))
+
+    def make_channel_map(self):
+        n = 2 ** int(self._d["toplevel_tree_rank"]) + 1
+        out = np.zeros(n, dtype=np.float64)
+        _check(lib().pb2_config_channel_map(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
+        return out
+
+    def delay_to_frequency(self, delay):
+        x = ctypes.c_double()
+        _check(lib().pb2_config_delay_to_frequency(self._h, float(delay), ctypes.byref(x)))
+        return x.value
+
+    def frequency_to_delay(self, freq):
+        x = ctypes.c_double()
+        _check(lib().pb2_config_frequency_to_delay(self._h, float(freq), ctypes.byref(x)))
+        return x.value
+
+    def dm_per_unit_delay(self):
+        x = ctypes.c_double()
+        _check(lib().pb2_config_dm_per_unit_delay(self._h, ctypes.byref(x)))
+        return x.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pb2_config_destroy(self._h)
+            self._h = None
+
+
+class DedispersionTree:
+    """Per-output-tree shapes (include/pirate/DedispersionTree.hpp:19-59)."""
+
+    def __init__(self, info):
+        for k, _ in _TreeInfo._fields_:
+            setattr(self, k, getattr(info, k))
+
+    def total_rank(self):
+        return self.amb_rank + self.dd_rank
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in _TreeInfo._fields_}
+
+
+class DedispersionPlan:
+    """pirate's DedispersionPlan (include/pirate/DedispersionPlan.hpp:33-225)."""
+
+    def __init__(self, config):
+        if isinstance(config, str):
+            config = DedispersionConfig.from_yaml(config)
+        self.config = config
+        h = ctypes.c_void_p()
+        _check(lib().pb2_plan_create(config._h, ctypes.byref(h)))
+        self._h = h
+        n = ctypes.c_long()
+        _check(lib().pb2_plan_ntrees(h, ctypes.byref(n)))
+        self.ntrees = n.value
+        self.trees = []
+        for i in range(self.ntrees):
+            info = _TreeInfo()
+            _check(lib().pb2_plan_tree_info(h, i, ctypes.byref(info)))
+            self.trees.append(DedispersionTree(info))
+        d = config.to_dict()
+        self.dtype = d["dtype"]
+        self.nfreq = config.get_total_nfreq()
+        self.nt_in = int(d["time_samples_per_chunk"])
+        self.num_primary_trees = len(d["primary_trees"])
+        self.beams_per_gpu = int(d["beams_per_gpu"])
+        self.beams_per_batch = int(d["beams_per_batch"])
+        self.num_active_batches = int(d["num_active_batches"])
+        npri = self.num_primary_trees
+        dd = (ctypes.c_long * npri)()
+        amb = (ctypes.c_long * npri)()
+        _check(lib().pb2_plan_stage1_ranks(h, dd, amb, npri))
+        self.stage1_dd_rank = list(dd)
+        self.stage1_amb_rank = list(amb)
+
+    def to_yaml_string(self):
+        return _yaml_out(lib().pb2_plan_to_yaml, self._h)
+
+    def decode_argmax(self, token, itree, idm, itime):
+        """Returns (fmin, fmax, tlo, thi, p) (src_lib/DedispersionPlan.cpp:481)."""
+        out = (ctypes.c_long * 5)()
+        _check(lib().pb2_plan_decode_argmax(self._h, int(token), int(itree), int(idm), int(itime), out))
+        return tuple(out)
+
+    def decode_argmax2(self, itree, fmin, fmax, tlo, thi, p):
+        """Returns (freq_lo_MHz, freq_hi_MHz, dm, timestamp_samp, width_samp) (src_lib/DedispersionPlan.cpp:544)."""
+        inp = (ctypes.c_long * 5)(fmin, fmax, tlo, thi, p)
+        out = (ctypes.c_double * 5)()
+        _check(lib().pb2_plan_decode_argmax2(self._h, int(itree), inp, out))
+        return tuple(out)
+
+    def compute_steady_state_it0(self, itree):
+        n = self.trees[itree].ndm_out
+        out = np.zeros(n, dtype=np.int64)
+        _check(lib().pb2_plan_steady_state_it0(self._h, int(itree), out.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), n))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pb2_plan_destroy(self._h)
+            self._h = None
+
+
+_TORCH_DTYPES = {0: "float32", 1: "float16", 2: "bfloat16"}
+
+
+def _device_tensor(ptr, shape, dtype, device):
+    """Wraps device memory owned by the dedisperser as a torch tensor (no copy)."""
+    import torch
+    tdt = getattr(torch, dtype)
+    n = int(np.prod(shape))
+    esize = torch.tensor([], dtype=tdt).element_size()
+    if n == 0:
+        return torch.empty(shape, dtype=tdt, device=device)
+    # Build a byte view via the CUDA array interface, then reinterpret.
+    holder = type("_Holder", (), {})()
+    holder.__cuda_array_interface__ = {"shape": (n * esize,), "typestr": "|u1", "data": (int(ptr), False), "version": 3}
+    t = torch.as_tensor(holder, device=device)
+    return t.view(tdt).view(*shape)
+
+
+class Outputs:
+    """GpuDedisperser::Outputs (include/pirate/Dedisperser.hpp:98-125); arrays are torch views."""
+
+    def __init__(self, o, device):
+        self.dtype = _TORCH_DTYPES[o.dtype]
+        self.nbeams = o.nbeams
+        self.ichunk_zero_based = o.ichunk_zero_based
+        self.ichunk_fpga_based = o.ichunk_fpga_based
+        self.ibeam = o.ibeam
+        self.ndm_out = [o.ndm_out[i] for i in range(o.ntrees)]
+        self.nt_out = [o.nt_out[i] for i in range(o.ntrees)]
+        self.out_max = [_device_tensor(o.out_max[i], (o.nbeams, o.ndm_out[i], o.nt_out[i]), self.dtype, device)
+                        for i in range(o.ntrees)]
+        # uint32 tokens, exposed as int32 views (same bits).
+        self.out_argmax = [_device_tensor(o.out_argmax[i], (o.nbeams, o.ndm_out[i], o.nt_out[i]), "int32", device)
+                           for i in range(o.ntrees)]
+
+
+class GpuDedisperser:
+    """pirate's GpuDedisperser (include/pirate/Dedisperser.hpp:45-254; python wrapper
+    pirate_frb/GpuDedisperser.py:123-197)."""
+
+    def __init__(self, plan, cuda_device_id=0, num_consumers=1, nbatches_out=0, nbatches_wt=0,
+                 initial_chunk=0, synchronous=True):
+        self.plan = plan
+        self.cuda_device_id = int(cuda_device_id)
+        self.device = "cuda:%d" % self.cuda_device_id
+        p = _DdParams(self.cuda_device_id, int(nbatches_out), int(nbatches_wt), int(num_consumers),
+                      1 if synchronous else 0, int(initial_chunk))
+        h = ctypes.c_void_p()
+        _check(lib().pb2_dd_create(plan._h, ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.num_consumers = int(num_consumers)
+        self.nbatches = plan.beams_per_gpu // plan.beams_per_batch
+        self.nbatches_out = int(nbatches_out) or plan.num_active_batches
+        self.nbatches_wt = int(nbatches_wt) or self.nbatches_out
+        self.dtype = plan.dtype
+        self._next_in = 0
+        self._next_out = [0] * self.num_consumers
+
+    def allocate(self):
+        _check(lib().pb2_dd_allocate(self._h))
+
+    def device_bytes(self):
+        n = ctypes.c_long()
+        _check(lib().pb2_dd_device_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def kernels_per_batch(self):
+        n = ctypes.c_long()
+        _check(lib().pb2_dd_kernels_per_batch(self._h, ctypes.byref(n)))
+        return n.value
+
+    def algorithmic_bytes(self):
+        """HBM bytes per (chunk, batch) for [grid, lds, stage1, stage2, pf]."""
+        out = (ctypes.c_double * 5)()
+        _check(lib().pb2_dd_algorithmic_bytes(self._h, out))
+        return list(out)
+
+    def acquire_input(self, seq_id, stream=None):
+        ptr = ctypes.c_void_p()
+        shape = (ctypes.c_long * 3)()
+        _check(lib().pb2_dd_acquire_input(self._h, int(seq_id), _stream_ptr(stream), ctypes.byref(ptr), shape))
+        return _device_tensor(ptr.value, tuple(shape), {"float32": "float32", "float16": "float16",
+                                                        "bfloat16": "bfloat16"}[self.dtype], self.device)
+
+    def release_input_and_launch_dd_kernels(self, seq_id, stream=None):
+        _check(lib().pb2_dd_release_input(self._h, int(seq_id), _stream_ptr(stream)))
+
+    def acquire_output(self, consumer_id, seq_id, stream=None, sync=False):
+        o = _Outputs()
+        _check(lib().pb2_dd_acquire_output(self._h, int(consumer_id), int(seq_id), _stream_ptr(stream),
+                                           1 if sync else 0, ctypes.byref(o)))
+        return Outputs(o, self.device)
+
+    def release_output(self, consumer_id, seq_id, stream=None):
+        _check(lib().pb2_dd_release_output(self._h, int(consumer_id), int(seq_id), _stream_ptr(stream)))
+
+    def fill_all_weights(self, itree, pf_weights):
+        """pf_weights: (nbatches_wt, beams_per_batch, ndm_wt, nt_wt, nprofiles, N) float32."""
+        w = np.ascontiguousarray(pf_weights, dtype=np.float32)
+        _check(lib().pb2_dd_fill_weights(self._h, int(itree), w.ctypes.data, w.size))
+
+    def stop(self):
+        _check(lib().pb2_dd_stop(self._h))
+
+    @contextlib.contextmanager
+    def get_input(self, stream=None):
+        """Context manager: yields the next input buffer, then launches the kernels on exit
+        (pirate_frb/GpuDedisperser.py:123-160)."""
+        seq = self._next_in
+        arr = self.acquire_input(seq, stream)
+        yield arr
+        self.release_input_and_launch_dd_kernels(seq, stream)
+        self._next_in += 1
+
+    @contextlib.contextmanager
+    def get_output(self, consumer_id=0, stream=None, sync=False):
+        """Context manager: yields the next Outputs for 'consumer_id', released on exit."""
+        seq = self._next_out[consumer_id]
+        out = self.acquire_output(consumer_id, seq, stream, sync)
+        yield out
+        self.release_output(consumer_id, seq, stream)
+        self._next_out[consumer_id] += 1
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pb2_dd_destroy(self._h)
+            self._h = None

@@ -1,0 +1,272 @@
+// capi.cpp -- extern "C" boundary (include/pirate_b200.h) over the C++ plan and GpuDedisperser.
+
+#include "../../include/pirate_b200.h"
+#include "dedisperser.hpp"
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+#include <memory>
+#include <string>
+
+using namespace pb2;
+
+struct pb2_config { DedispersionConfig c; };
+struct pb2_plan { std::shared_ptr<DedispersionPlan> p; };
+struct pb2_dedisperser { std::unique_ptr<GpuDedisperser> d; };
+
+static thread_local std::string g_err;
+
+template<typename F>
+static int guard(F &&f)
+{
+    try {
+        f();
+        g_err.clear();
+        return 0;
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return 1;
+    } catch (...) {
+        g_err = "unknown error";
+        return 1;
+    }
+}
+
+static void copy_out(const std::string &s, char *buf, long buflen, long *needed)
+{
+    if (needed) *needed = long(s.size()) + 1;
+    if (buf && buflen > 0) {
+        long n = std::min(long(s.size()), buflen - 1);
+        memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+}
+
+#define REQUIRE_PTR(p) do { if (!(p)) throw std::runtime_error(std::string(__func__) + ": null argument '" #p "'"); } while (0)
+
+extern "C" {
+
+const char *pb2_last_error(void) { return g_err.c_str(); }
+const char *pb2_version(void) { return "pirate_b200 0.1 (sm_100a)"; }
+
+int pb2_config_from_yaml(const char *path, pb2_config **out)
+{
+    return guard([&] { REQUIRE_PTR(path); REQUIRE_PTR(out); *out = new pb2_config{DedispersionConfig::from_yaml(path)}; });
+}
+
+int pb2_config_from_yaml_string(const char *text, pb2_config **out)
+{
+    return guard([&] { REQUIRE_PTR(text); REQUIRE_PTR(out); *out = new pb2_config{DedispersionConfig::from_yaml_string(text, "yaml")}; });
+}
+
+int pb2_config_to_yaml(const pb2_config *cfg, char *buf, long buflen, long *needed)
+{
+    return guard([&] { REQUIRE_PTR(cfg); copy_out(cfg->c.to_yaml_string(), buf, buflen, needed); });
+}
+
+int pb2_config_channel_map(const pb2_config *cfg, double *out, long n)
+{
+    return guard([&] {
+        REQUIRE_PTR(cfg); REQUIRE_PTR(out);
+        std::vector<double> cm = cfg->c.make_channel_map();
+        if (n != (long) cm.size()) throw std::runtime_error("pb2_config_channel_map: expected n=" + std::to_string(cm.size()));
+        memcpy(out, cm.data(), cm.size() * sizeof(double));
+    });
+}
+
+int pb2_config_delay_to_frequency(const pb2_config *cfg, double delay, double *freq)
+{
+    return guard([&] { REQUIRE_PTR(cfg); REQUIRE_PTR(freq); *freq = cfg->c.delay_to_frequency(delay); });
+}
+
+int pb2_config_frequency_to_delay(const pb2_config *cfg, double freq, double *delay)
+{
+    return guard([&] { REQUIRE_PTR(cfg); REQUIRE_PTR(delay); *delay = cfg->c.frequency_to_delay(freq); });
+}
+
+int pb2_config_dm_per_unit_delay(const pb2_config *cfg, double *dm)
+{
+    return guard([&] { REQUIRE_PTR(cfg); REQUIRE_PTR(dm); *dm = cfg->c.dm_per_unit_delay(); });
+}
+
+void pb2_config_destroy(pb2_config *cfg) { delete cfg; }
+
+int pb2_plan_create(const pb2_config *cfg, pb2_plan **out)
+{
+    return guard([&] { REQUIRE_PTR(cfg); REQUIRE_PTR(out); *out = new pb2_plan{std::make_shared<DedispersionPlan>(cfg->c)}; });
+}
+
+void pb2_plan_destroy(pb2_plan *plan) { delete plan; }
+
+int pb2_plan_to_yaml(const pb2_plan *plan, char *buf, long buflen, long *needed)
+{
+    return guard([&] { REQUIRE_PTR(plan); copy_out(plan->p->to_yaml_string(), buf, buflen, needed); });
+}
+
+int pb2_plan_ntrees(const pb2_plan *plan, long *ntrees)
+{
+    return guard([&] { REQUIRE_PTR(plan); REQUIRE_PTR(ntrees); *ntrees = plan->p->ntrees; });
+}
+
+int pb2_plan_tree_info(const pb2_plan *plan, long itree, pb2_tree_info *o)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(o);
+        if (itree < 0 || itree >= plan->p->ntrees) throw std::runtime_error("pb2_plan_tree_info: itree out of range");
+        const DedispersionTree &t = plan->p->trees[itree];
+        o->primary_tree_index = t.primary_tree_index;
+        o->early_trigger_level = t.early_trigger_level;
+        o->amb_rank = t.amb_rank;
+        o->dd_rank = t.dd_rank;
+        o->nt_ds = t.nt_ds;
+        o->ndm_out = t.ndm_out;
+        o->nt_out = t.nt_out;
+        o->ndm_wt = t.ndm_wt;
+        o->nt_wt = t.nt_wt;
+        o->nprofiles = t.nprofiles;
+        o->Dcore = t.Dcore;
+        o->max_width = t.pf.max_width;
+        o->dm_downsampling = t.pf.dm_downsampling;
+        o->time_downsampling = t.pf.time_downsampling;
+        o->wt_dm_downsampling = t.pf.wt_dm_downsampling;
+        o->wt_time_downsampling = t.pf.wt_time_downsampling;
+        o->nsubbands = t.frequency_subbands.N;
+        o->nmultiplets = t.frequency_subbands.M;
+        o->pf_rank = t.frequency_subbands.pf_rank;
+        o->dm_min = t.dm_min;
+        o->dm_max = t.dm_max;
+        o->trigger_frequency = t.trigger_frequency;
+    });
+}
+
+int pb2_plan_stage1_ranks(const pb2_plan *plan, long *dd_rank, long *amb_rank, long n)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(dd_rank); REQUIRE_PTR(amb_rank);
+        if (n != plan->p->num_primary_trees) throw std::runtime_error("pb2_plan_stage1_ranks: n must equal num_primary_trees");
+        for (long i = 0; i < n; i++) { dd_rank[i] = plan->p->stage1_dd_rank[i]; amb_rank[i] = plan->p->stage1_amb_rank[i]; }
+    });
+}
+
+int pb2_plan_decode_argmax(const pb2_plan *plan, uint32_t token, long itree, long idm, long itime, long *o)
+{
+    return guard([&] { REQUIRE_PTR(plan); REQUIRE_PTR(o); plan->p->decode_argmax(token, itree, idm, itime, o[0], o[1], o[2], o[3], o[4]); });
+}
+
+int pb2_plan_decode_argmax2(const pb2_plan *plan, long itree, const long *in5, double *o)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(in5); REQUIRE_PTR(o);
+        plan->p->decode_argmax2(itree, in5[0], in5[1], in5[2], in5[3], in5[4], o[0], o[1], o[2], o[3], o[4]);
+    });
+}
+
+int pb2_plan_steady_state_it0(const pb2_plan *plan, long itree, long *out, long n)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(out);
+        std::vector<long> v = plan->p->compute_steady_state_it0(itree);
+        if (n != (long) v.size()) throw std::runtime_error("pb2_plan_steady_state_it0: n must equal ndm_out");
+        memcpy(out, v.data(), v.size() * sizeof(long));
+    });
+}
+
+int pb2_dd_create(const pb2_plan *plan, const pb2_dd_params *p, pb2_dedisperser **out)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(p); REQUIRE_PTR(out);
+        if (plan->p->ntrees > PB2_MAX_TREES) throw std::runtime_error("pb2_dd_create: too many trees");
+        GpuDedisperser::Params gp;
+        gp.cuda_device_id = p->cuda_device_id;
+        gp.nbatches_out = p->nbatches_out;
+        gp.nbatches_wt = p->nbatches_wt;
+        gp.num_consumers = p->num_consumers;
+        gp.synchronous = p->synchronous != 0;
+        gp.initial_chunk = p->initial_chunk;
+        *out = new pb2_dedisperser{std::unique_ptr<GpuDedisperser>(new GpuDedisperser(*plan->p, gp))};
+    });
+}
+
+int pb2_dd_allocate(pb2_dedisperser *dd)
+{
+    return guard([&] { REQUIRE_PTR(dd); dd->d->allocate(); });
+}
+
+int pb2_dd_device_bytes(const pb2_dedisperser *dd, long *nbytes)
+{
+    return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(nbytes); *nbytes = long(dd->d->device_bytes()); });
+}
+
+int pb2_dd_acquire_input(pb2_dedisperser *dd, long seq_id, void *stream, void **ptr, long *shape3)
+{
+    return guard([&] {
+        REQUIRE_PTR(dd); REQUIRE_PTR(ptr);
+        *ptr = dd->d->acquire_input(seq_id, (cudaStream_t) stream);
+        if (shape3) {
+            shape3[0] = dd->d->plan.beams_per_batch;
+            shape3[1] = dd->d->plan.nfreq;
+            shape3[2] = dd->d->plan.nt_in;
+        }
+    });
+}
+
+int pb2_dd_release_input(pb2_dedisperser *dd, long seq_id, void *stream)
+{
+    return guard([&] { REQUIRE_PTR(dd); dd->d->release_input_and_launch_dd_kernels(seq_id, (cudaStream_t) stream); });
+}
+
+int pb2_dd_acquire_output(pb2_dedisperser *dd, long consumer_id, long seq_id, void *stream, int sync, pb2_outputs *out)
+{
+    return guard([&] {
+        REQUIRE_PTR(dd); REQUIRE_PTR(out);
+        GpuDedisperser::Outputs o = dd->d->acquire_output(consumer_id, seq_id, (cudaStream_t) stream, sync != 0);
+        memset(out, 0, sizeof(*out));
+        out->dtype = int(o.dtype);
+        out->nbeams = o.nbeams;
+        out->ichunk_zero_based = o.ichunk_zero_based;
+        out->ichunk_fpga_based = o.ichunk_fpga_based;
+        out->ibeam = o.ibeam;
+        out->ntrees = long(o.out_max.size());
+        for (size_t i = 0; i < o.out_max.size(); i++) {
+            out->ndm_out[i] = o.ndm_out[i];
+            out->nt_out[i] = o.nt_out[i];
+            out->out_max[i] = o.out_max[i];
+            out->out_argmax[i] = o.out_argmax[i];
+        }
+    });
+}
+
+int pb2_dd_release_output(pb2_dedisperser *dd, long consumer_id, long seq_id, void *stream)
+{
+    return guard([&] { REQUIRE_PTR(dd); dd->d->release_output(consumer_id, seq_id, (cudaStream_t) stream); });
+}
+
+int pb2_dd_fill_weights(pb2_dedisperser *dd, long itree, const float *host, long nelts)
+{
+    return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(host); dd->d->fill_all_weights(itree, host, nelts); });
+}
+
+int pb2_dd_stop(pb2_dedisperser *dd)
+{
+    return guard([&] { REQUIRE_PTR(dd); dd->d->stop(); });
+}
+
+int pb2_dd_kernels_per_batch(const pb2_dedisperser *dd, long *n)
+{
+    return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(n); *n = dd->d->kernels_per_batch(); });
+}
+
+int pb2_dd_algorithmic_bytes(const pb2_dedisperser *dd, double *out5)
+{
+    return guard([&] {
+        REQUIRE_PTR(dd); REQUIRE_PTR(out5);
+        std::vector<double> v = dd->d->algorithmic_bytes();
+        for (int i = 0; i < 5; i++) out5[i] = v[i];
+    });
+}
+
+void pb2_dd_destroy(pb2_dedisperser *dd) { delete dd; }
+
+}  // extern "C"

@@ -1,0 +1,621 @@
+// dedisperser.cu -- host driver of the B200 dedispersion path (see dedisperser.hpp).
+
+#include "dedisperser.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+
+namespace pb2 {
+
+using std::runtime_error;
+using std::vector;
+
+#define CUDA_CHECK(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { \
+    std::stringstream _ss; _ss << #x << ": " << cudaGetErrorString(_e); throw runtime_error(_ss.str()); } } while (0)
+
+static long next_pow2(long n) { long p = 1; while (p < n) p <<= 1; return p; }
+static long round_up(long n, long k) { return ((n + k - 1) / k) * k; }
+
+
+DeviceBuffer::~DeviceBuffer() { if (ptr) cudaFree(ptr); }
+
+void DeviceBuffer::alloc(size_t n)
+{
+    if (ptr) { cudaFree(ptr); ptr = nullptr; }
+    nbytes = n;
+    if (n == 0) return;
+    CUDA_CHECK(cudaMalloc(&ptr, n));
+    CUDA_CHECK(cudaMemset(ptr, 0, n));
+}
+
+void DeviceBuffer::upload(const void *host, size_t n)
+{
+    alloc(n);
+    if (n) CUDA_CHECK(cudaMemcpy(ptr, host, n, cudaMemcpyHostToDevice));
+}
+
+
+// -------------------------------------------------------------------------------------------------
+// Tree programs.
+//
+// Stage 1 (src_lib/ReferenceTree.cpp:120-300 with no subbands): step r pairs rows i and i + 2^r
+// (i = fo * 2^(r+1) + j, j < 2^r) with lag bit_reverse(j, r).
+//
+// Stage 2 follows ReferenceTree::dedisperse_2d (src_lib/ReferenceTree.cpp:120-300) step by step:
+// pf-level-0 subbands are copies of the current rows; staggered subbands at pf_level > 0 are
+// butterflies over band pairs (pfs, pfs+1) whose even members coincide with in-place butterflies.
+
+
+static TreeOp make_bfly(int row0, int row1, int lag, int kind, long &hoff)
+{
+    TreeOp op;
+    op.row0 = int16_t(row0);
+    op.row1 = int16_t(row1);
+    op.kind = int16_t(kind);
+    op.pad = 0;
+    op.lag = lag;
+    long cap = next_pow2(lag + 1);
+    op.hist_off = int32_t(hoff);
+    op.hist_mask = int32_t(cap - 1);
+    hoff += cap;
+    op.out0 = op.out1 = -1;
+    return op;
+}
+
+TreeProgram make_stage1_program(int R)
+{
+    TreeProgram P;
+    long hoff = 0;
+    for (int r = 0; r < R; r++) {
+        P.phase_begin.push_back(P.ops.size());
+        int ndm_in = 1 << r;
+        for (int fo = 0; fo < (1 << (R - r - 1)); fo++)
+            for (int j = 0; j < ndm_in; j++) {
+                int row0 = fo * 2 * ndm_in + j;
+                P.ops.push_back(make_bfly(row0, row0 + ndm_in, bit_reverse(j, r), 0, hoff));
+            }
+    }
+    P.phase_begin.push_back(P.ops.size());
+    P.hist_per_block = hoff;
+    P.nsteps = R;
+    P.nout = 0;
+    return P;
+}
+
+TreeProgram make_stage2_program(int R, const FrequencySubbands &fs)
+{
+    TreeProgram P;
+    const int pf_rank = fs.pf_rank, M = fs.M, pf_ndm = 1 << (R - pf_rank);
+    if (pf_rank > R) throw runtime_error("make_stage2_program: pf_rank > dd_rank");
+    long hoff = 0;
+    int mcurr = 0;
+
+    for (int r = 0; r <= R; r++) {
+        int ndm_in = 1 << r;
+        vector<TreeOp> copies, stag, tree;
+
+        if (r == R - pf_rank) {
+            int pf_ns = fs.subband_counts[0];
+            for (int dm_in = 0; dm_in < ndm_in; dm_in++) {
+                int dbr = bit_reverse(dm_in, r);
+                for (int pfs = 0; pfs < pf_ns; pfs++) {
+                    TreeOp op;
+                    memset(&op, 0, sizeof(op));
+                    op.kind = 2;
+                    op.row0 = int16_t(pfs * ndm_in + dbr);
+                    op.row1 = op.row0;
+                    op.out0 = dm_in * M + mcurr + pfs;
+                    op.out1 = -1;
+                    copies.push_back(op);
+                }
+            }
+            mcurr += pf_ns;
+        }
+
+        if (r < R) {
+            for (int fo = 0; fo < (1 << (R - r - 1)); fo++)
+                for (int j = 0; j < ndm_in; j++) {
+                    int row0 = fo * 2 * ndm_in + j;
+                    tree.push_back(make_bfly(row0, row0 + ndm_in, bit_reverse(j, r), 0, hoff));
+                }
+            int pf_level = r + pf_rank - R + 1;
+            if (pf_level > 0) {
+                int pf_ns = fs.subband_counts[pf_level], pf_nd2 = 1 << (pf_level - 1);
+                if (ndm_in != pf_ndm * pf_nd2) throw runtime_error("make_stage2_program: inconsistent subband shape");
+                for (int pf_dm = 0; pf_dm < pf_ndm; pf_dm++)
+                    for (int d2 = 0; d2 < pf_nd2; d2++) {
+                        int dm_in = pf_dm * pf_nd2 + d2;
+                        int dbr = bit_reverse(dm_in, r);
+                        for (int pfs = 0; pfs < pf_ns; pfs++) {
+                            int m = mcurr + pfs * 2 * pf_nd2 + 2 * d2;
+                            int o0 = pf_dm * M + m;
+                            if ((pfs & 1) == 0) {
+                                TreeOp &op = tree.at((pfs / 2) * ndm_in + dbr);
+                                if (op.lag != dm_in || op.row0 != pfs * ndm_in + dbr) throw runtime_error("make_stage2_program: pairing mismatch");
+                                op.out0 = o0;
+                                op.out1 = o0 + 1;
+                            }
+                            else {
+                                int row0 = pfs * ndm_in + dbr;
+                                TreeOp op = make_bfly(row0, row0 + ndm_in, dm_in, 1, hoff);
+                                op.out0 = o0;
+                                op.out1 = o0 + 1;
+                                stag.push_back(op);
+                            }
+                        }
+                    }
+                mcurr += pf_ns * 2 * pf_nd2;
+            }
+        }
+
+        if (r < R || !copies.empty()) {
+            P.phase_begin.push_back(P.ops.size());
+            P.ops.insert(P.ops.end(), copies.begin(), copies.end());
+            P.ops.insert(P.ops.end(), stag.begin(), stag.end());
+            P.ops.insert(P.ops.end(), tree.begin(), tree.end());
+        }
+    }
+    P.phase_begin.push_back(P.ops.size());
+    if (mcurr != M) throw runtime_error("make_stage2_program: multiplet count mismatch");
+
+    // Every subband output row must be produced exactly once per tile.
+    P.nout = pf_ndm * M;
+    vector<int> seen(P.nout, 0);
+    for (const TreeOp &op : P.ops) {
+        if (op.out0 >= 0) seen.at(op.out0)++;
+        if (op.out1 >= 0) seen.at(op.out1)++;
+    }
+    for (int c : seen)
+        if (c != 1) throw runtime_error("make_stage2_program: subband outputs not covered exactly once");
+
+    P.hist_per_block = hoff;
+    P.nsteps = R;
+    return P;
+}
+
+
+// -------------------------------------------------------------------------------------------------
+// GpuDedisperser
+
+
+GpuDedisperser::GpuDedisperser(const DedispersionPlan &plan_, const Params &params_) : plan(plan_), params(params_)
+{
+    B = plan.beams_per_batch;
+    total_beams = plan.beams_per_gpu;
+    nbatches = total_beams / B;
+    nslots_in = plan.num_active_batches;
+    nbatches_out = params.nbatches_out ? params.nbatches_out : plan.num_active_batches;
+    nbatches_wt = params.nbatches_wt ? params.nbatches_wt : nbatches_out;
+    if (params.num_consumers < 0) throw runtime_error("GpuDedisperser: num_consumers must be >= 0");
+    if (params.cuda_device_id < 0) throw runtime_error("GpuDedisperser: cuda_device_id must be >= 0");
+    if (nbatches_out <= 0 || nbatches_wt <= 0) throw runtime_error("GpuDedisperser: nbatches_out/nbatches_wt must be > 0");
+    dtype_code = int(plan.dtype);
+    esize = (plan.dtype == Dtype::f32) ? 4 : 2;
+    next_acq_out.assign(params.num_consumers, 0);
+    next_rel_out.assign(params.num_consumers, 0);
+}
+
+GpuDedisperser::~GpuDedisperser()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaSetDevice(params.cuda_device_id);
+    if (compute) cudaStreamSynchronize(compute);
+    auto kill = [](vector<cudaEvent_t> &v) { for (cudaEvent_t e : v) if (e) cudaEventDestroy(e); v.clear(); };
+    kill(ev_in_acquired);
+    kill(ev_in_free);
+    kill(ev_out_done);
+    for (auto &v : ev_out_released) kill(v);
+    if (compute) cudaStreamDestroy(compute);
+    cudaSetDevice(dev);
+}
+
+void GpuDedisperser::check_alive() const
+{
+    if (error) std::rethrow_exception(error);
+    if (stopped) throw runtime_error("GpuDedisperser: entry point called after stop()");
+}
+
+template<typename F>
+auto GpuDedisperser::entry(F &&f) -> decltype(f())
+{
+    std::lock_guard<std::mutex> lk(mtx);
+    check_alive();
+    try {
+        return f();
+    } catch (...) {
+        error = std::current_exception();
+        stopped = true;
+        throw;
+    }
+}
+
+void GpuDedisperser::stop(std::exception_ptr e)
+{
+    std::lock_guard<std::mutex> lk(mtx);
+    if (!error && e) error = e;
+    stopped = true;
+}
+
+int GpuDedisperser::kernels_per_batch() const
+{
+    return 1 + (plan.num_primary_trees > 1 ? 1 : 0) + int(plan.num_primary_trees) + 2 * int(plan.ntrees);
+}
+
+std::vector<double> GpuDedisperser::algorithmic_bytes() const
+{
+    // Compulsory bytes each kernel must move per (chunk, batch): every element it reads or writes
+    // once (the reference's ResourceTracker model, src_lib/TreeGriddingKernel.cu:117,
+    // GpuLaggedDownsamplingKernel.cu:767-774, DedispersionKernel.cu:514-516, CoalescedDdKernel2.cu:128-135).
+    double S = double(esize);
+    long rank = plan.config.toplevel_tree_rank, nt = plan.nt_in;
+    double grid = double(B) * (plan.nfreq + pow2(rank)) * nt * S;
+    double lds = 0, st1 = 0, st2 = 0, pf = 0;
+    if (plan.num_primary_trees > 1) {
+        lds += double(B) * pow2(rank) * nt * S;
+        for (long p = 1; p < plan.num_primary_trees; p++) lds += double(B) * pow2(rank - 1) * (nt >> p) * S;
+    }
+    for (long p = 0; p < plan.num_primary_trees; p++) {
+        long rk = plan.stage1_dd_rank[p] + plan.stage1_amb_rank[p];
+        st1 += 2.0 * B * pow2(rk) * (nt >> p) * S;
+    }
+    for (const DedispersionTree &t : plan.trees) {
+        long M = t.frequency_subbands.M;
+        st2 += double(B) * pow2(t.total_rank()) * t.nt_ds * S + double(B) * t.ndm_out * M * t.nt_ds * S;
+        pf += double(B) * t.ndm_out * M * t.nt_ds * S + double(B) * t.ndm_out * t.nt_out * (S + 4);
+    }
+    return {grid, lds, st1, st2, pf};
+}
+
+void GpuDedisperser::allocate()
+{
+    entry([&]() {
+        if (allocated) throw runtime_error("GpuDedisperser::allocate() called twice");
+        CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
+        CUDA_CHECK(cudaStreamCreateWithFlags(&compute, cudaStreamNonBlocking));
+        auto mk = [](vector<cudaEvent_t> &v, long n) {
+            v.resize(n);
+            for (auto &e : v) CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        };
+        mk(ev_in_acquired, nslots_in);
+        mk(ev_in_free, nslots_in);
+        mk(ev_out_done, nbatches_out);
+        ev_out_released.resize(params.num_consumers);
+        for (auto &v : ev_out_released) mk(v, nbatches_out);
+        in_free_recorded.assign(nslots_in, false);
+        out_done_recorded.assign(nbatches_out, false);
+        out_released_recorded.assign(params.num_consumers, vector<bool>(nbatches_out, false));
+
+        const long rank = plan.config.toplevel_tree_rank, nt = plan.nt_in, F = plan.nfreq, N = pow2(rank);
+        const long npri = plan.num_primary_trees;
+        total_bytes = 0;
+        auto add = [&](DeviceBuffer &d, size_t n) { d.alloc(n); total_bytes += n; };
+
+        // Tree gridding table (src_lib/TreeGriddingKernel.cu:80-97): channel n covers input channels
+        // [floor(cm[n+1]), floor(cm[n])] with overlap weights float(w) in ascending order.
+        vector<double> cm = plan.config.make_channel_map();
+        vector<int> f0(N), cnt(N), woff(N);
+        vector<float> w;
+        for (long n = 0; n < N; n++) {
+            double a0 = cm[n + 1], a1 = cm[n];
+            long if0 = std::max(long(a0), 0L), if1 = std::min(long(a1) + 1, F);
+            f0[n] = int(if0);
+            cnt[n] = int(std::max(if1 - if0, 0L));
+            woff[n] = int(w.size());
+            for (long f = if0; f < if1; f++) {
+                double lo = std::max(a0, double(f)), hi = std::min(a1, double(f) + 1);
+                w.push_back(float(std::max(hi - lo, 0.0)));
+            }
+        }
+        d_grid_f0.upload(f0.data(), f0.size() * 4);
+        d_grid_cnt.upload(cnt.data(), cnt.size() * 4);
+        d_grid_woff.upload(woff.data(), woff.size() * 4);
+        d_grid_w.upload(w.data(), w.size() * 4);
+
+        add(d_inputs, size_t(nslots_in) * B * F * nt * esize);
+        add(d_tree0, size_t(B) * N * nt * esize);
+        if (npri > 1) add(d_lds_state, size_t(2) * total_beams * (npri - 1) * (N / 2) * sizeof(float));
+
+        s1.clear();
+        s1.resize(npri);
+        for (long p = 0; p < npri; p++) {
+            Stage1 &st = s1[p];
+            int R1 = plan.stage1_dd_rank[p], A1 = plan.stage1_amb_rank[p];
+            st.prog = make_stage1_program(R1);
+            st.nblocks = 1 << A1;
+            st.nt = int(nt >> p);
+            st.ops.upload(st.prog.ops.data(), st.prog.ops.size() * sizeof(TreeOp));
+            st.phases.upload(st.prog.phase_begin.data(), st.prog.phase_begin.size() * sizeof(int));
+            add(st.hist, size_t(total_beams) * st.nblocks * st.prog.hist_per_block * sizeof(float));
+
+            long nrows = pow2(R1 + A1);
+            vector<long> off(nrows);
+            vector<int> cap(nrows);
+            long tot = 0;
+            for (long row = 0; row < nrows; row++) {
+                cap[row] = int(round_up(plan.max_row_lag[p][row] + st.nt, 32));
+                off[row] = tot;
+                tot += cap[row];
+            }
+            st.ring_beam_stride = tot;
+            st.ring_off.upload(off.data(), off.size() * sizeof(long));
+            st.ring_cap.upload(cap.data(), cap.size() * sizeof(int));
+            add(st.ring, size_t(total_beams) * tot * esize);
+
+            if (p > 0) {
+                st.lds_cap = next_pow2(st.nt + (1L << R1) - 1);
+                add(st.lds, size_t(total_beams) * (N / 2) * st.lds_cap * esize);
+            }
+        }
+
+        s2.clear();
+        s2.resize(plan.ntrees);
+        for (long i = 0; i < plan.ntrees; i++) {
+            const DedispersionTree &t = plan.trees[i];
+            Stage2 &st = s2[i];
+            const FrequencySubbands &fs = t.frequency_subbands;
+            st.prog = make_stage2_program(t.dd_rank, fs);
+            st.nblocks = 1 << t.amb_rank;
+            st.M = fs.M;
+            st.N = fs.N;
+            st.P = t.nprofiles;
+            st.L = std::max(integer_log2(t.pf.max_width), 1);
+            st.tpad = int(std::max(2 * t.pf.max_width, 4L));
+            st.pf_shift = t.dd_rank - fs.pf_rank;
+            st.Dout = int(t.pf.time_downsampling);
+            st.ops.upload(st.prog.ops.data(), st.prog.ops.size() * sizeof(TreeOp));
+            st.phases.upload(st.prog.phase_begin.data(), st.prog.phase_begin.size() * sizeof(int));
+            add(st.hist, size_t(total_beams) * st.nblocks * st.prog.hist_per_block * sizeof(float));
+
+            // Subband alignment lag of (pf_dm, m): (2^pf_rank - fhi(m)) * pf_dm (src_lib/ReferenceTree.cpp:41-50).
+            int npfdm = 1 << st.pf_shift;
+            vector<int> fl(npfdm * st.M), m2n(st.M);
+            long maxlag = 0;
+            for (int d = 0; d < npfdm; d++)
+                for (int m = 0; m < st.M; m++) {
+                    long lag = (pow2(fs.pf_rank) - fs.m_to_fhi(m)) * d;
+                    fl[d * st.M + m] = int(lag);
+                    maxlag = std::max(maxlag, lag);
+                }
+            for (int m = 0; m < st.M; m++) m2n[m] = int(fs.m_to_n[m]);
+            st.final_lag.upload(fl.data(), fl.size() * sizeof(int));
+            st.m_to_n.upload(m2n.data(), m2n.size() * sizeof(int));
+            st.pf_cap = next_pow2(t.nt_ds + st.tpad + maxlag + st.Dout);
+            add(st.pfring, size_t(total_beams) * t.ndm_out * st.M * st.pf_cap * esize);
+            add(st.out_max, size_t(nbatches_out) * B * t.ndm_out * t.nt_out * esize);
+            add(st.out_argmax, size_t(nbatches_out) * B * t.ndm_out * t.nt_out * sizeof(uint32_t));
+            add(st.wt, size_t(nbatches_wt) * B * t.ndm_wt * t.nt_wt * t.nprofiles * fs.N * sizeof(float));
+        }
+        CUDA_CHECK(cudaDeviceSynchronize());
+        allocated = true;
+    });
+}
+
+void *GpuDedisperser::acquire_input(long seq_id, cudaStream_t stream)
+{
+    return entry([&]() -> void * {
+        if (!allocated) throw runtime_error("GpuDedisperser::acquire_input(): allocate() was not called");
+        if (seq_id != next_acq_in)
+            throw runtime_error("GpuDedisperser::acquire_input(): expected seq_id=" + std::to_string(next_acq_in) + ", got " + std::to_string(seq_id));
+        long slot = seq_id % nslots_in;
+        if (in_free_recorded[slot]) CUDA_CHECK(cudaStreamWaitEvent(stream, ev_in_free[slot], 0));
+        next_acq_in++;
+        return d_inputs.as<char>() + size_t(slot) * B * plan.nfreq * plan.nt_in * esize;
+    });
+}
+
+void GpuDedisperser::release_input_and_launch_dd_kernels(long seq_id, cudaStream_t stream)
+{
+    entry([&]() {
+        if (seq_id != next_rel_in || seq_id >= next_acq_in)
+            throw runtime_error("GpuDedisperser::release_input_and_launch_dd_kernels(): expected seq_id=" + std::to_string(next_rel_in) + ", got " + std::to_string(seq_id));
+        long slot = seq_id % nslots_in;
+        CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
+        CUDA_CHECK(cudaEventRecord(ev_in_acquired[slot], stream));
+        CUDA_CHECK(cudaStreamWaitEvent(compute, ev_in_acquired[slot], 0));
+        launch_batch(seq_id);
+        next_rel_in++;
+    });
+}
+
+void GpuDedisperser::launch_batch(long seq_id)
+{
+    const long ichunk = seq_id / nbatches, ibatch = seq_id % nbatches;
+    const long slot_in = seq_id % nslots_in, slot_out = seq_id % nbatches_out, slot_wt = seq_id % nbatches_wt;
+    const long rank = plan.config.toplevel_tree_rank, nt = plan.nt_in, F = plan.nfreq, N = pow2(rank);
+    const long npri = plan.num_primary_trees;
+    const int beam0 = int(ibatch * B);
+    cudaStream_t s = compute;
+
+    GridArgs g;
+    g.in = d_inputs.as<char>() + size_t(slot_in) * B * F * nt * esize;
+    g.out = d_tree0.ptr;
+    g.chan_f0 = d_grid_f0.as<int>();
+    g.chan_cnt = d_grid_cnt.as<int>();
+    g.chan_woff = d_grid_woff.as<int>();
+    g.chan_w = d_grid_w.as<float>();
+    g.F = int(F); g.N = int(N); g.T = int(nt);
+    launch_grid(g, dtype_code, int(B), s);
+    CUDA_CHECK(cudaEventRecord(ev_in_free[slot_in], s));
+    in_free_recorded[slot_in] = true;
+
+    if (npri > 1) {
+        LdsArgs l;
+        memset(&l, 0, sizeof(l));
+        l.in = d_tree0.ptr;
+        l.rank = int(rank); l.T = int(nt); l.nlev = int(npri - 1);
+        for (long p = 1; p < npri; p++) {
+            l.ring[p - 1] = s1[p].lds.ptr;
+            l.cap_mask[p - 1] = s1[p].lds_cap - 1;
+        }
+        l.state = d_lds_state.as<float>();
+        l.ichunk = ichunk;
+        l.beam0 = beam0; l.B = int(B); l.total_beams = int(total_beams);
+        launch_lds(l, dtype_code, s);
+    }
+
+    for (long p = 0; p < npri; p++) {
+        Stage1 &st = s1[p];
+        Stage1Args a;
+        memset(&a, 0, sizeof(a));
+        a.ops = st.ops.as<TreeOp>();
+        a.phase_begin = st.phases.as<int>();
+        a.nphases = int(st.prog.phase_begin.size() - 1);
+        a.nrows = 1 << plan.stage1_dd_rank[p];
+        a.hist_per_block = st.prog.hist_per_block;
+        a.hist = st.hist.as<float>();
+        if (p == 0) {
+            a.in = d_tree0.ptr;
+            a.in_beam_stride = N * nt;
+            a.in_row_stride = nt;
+            a.in_mask = -1;
+            a.in_s0 = 0;
+            a.in_lag0 = a.in_lag1 = 0;
+            a.in_beam0 = 0;
+        } else {
+            a.in = st.lds.ptr;
+            a.in_beam_stride = (N / 2) * st.lds_cap;
+            a.in_row_stride = st.lds_cap;
+            a.in_mask = st.lds_cap - 1;
+            a.in_s0 = ichunk * st.nt;
+            a.in_lag0 = (1 << plan.stage1_dd_rank[p]) - 1;   // lag 2^s1dd - 1 - j (ReferenceLaggedDownsamplingKernel.cpp:53-55)
+            a.in_lag1 = 1;
+            a.in_beam0 = beam0;
+        }
+        a.ring = st.ring.ptr;
+        a.ring_off = st.ring_off.as<long>();
+        a.ring_cap = st.ring_cap.as<int>();
+        a.ring_beam_stride = st.ring_beam_stride;
+        a.s0 = ichunk * st.nt;
+        a.nt = st.nt;
+        a.beam0 = beam0;
+        launch_stage1(a, dtype_code, st.nblocks, int(B), s);
+    }
+
+    for (long i = 0; i < plan.ntrees; i++) {
+        const DedispersionTree &t = plan.trees[i];
+        Stage2 &st = s2[i];
+        Stage1 &src = s1[t.primary_tree_index];
+        Stage2Args a;
+        memset(&a, 0, sizeof(a));
+        a.ops = st.ops.as<TreeOp>();
+        a.phase_begin = st.phases.as<int>();
+        a.nphases = int(st.prog.phase_begin.size() - 1);
+        a.nrows = 1 << t.dd_rank;
+        a.hist_per_block = st.prog.hist_per_block;
+        a.hist = st.hist.as<float>();
+        a.ring = src.ring.ptr;
+        a.ring_off = src.ring_off.as<long>();
+        a.ring_cap = src.ring_cap.as<int>();
+        a.ring_beam_stride = src.ring_beam_stride;
+        a.amb_rank = t.amb_rank;
+        a.dd_rank = t.dd_rank;
+        a.uflag = (t.primary_tree_index > 0) ? 1 : 0;
+        a.pf = st.pfring.ptr;
+        a.M = st.M;
+        a.ndm_out = int(t.ndm_out);
+        a.pf_shift = st.pf_shift;
+        a.pf_cap = st.pf_cap;
+        a.s0 = ichunk * t.nt_ds;
+        a.nt = t.nt_ds;
+        a.beam0 = beam0;
+        launch_stage2(a, dtype_code, st.nblocks, int(B), s);
+    }
+
+    // Output back-pressure: slot_out is reusable once every consumer released seq_id - nbatches_out.
+    for (long c = 0; c < params.num_consumers; c++)
+        if (out_released_recorded[c][slot_out])
+            CUDA_CHECK(cudaStreamWaitEvent(s, ev_out_released[c][slot_out], 0));
+
+    for (long i = 0; i < plan.ntrees; i++) {
+        const DedispersionTree &t = plan.trees[i];
+        Stage2 &st = s2[i];
+        PfArgs a;
+        memset(&a, 0, sizeof(a));
+        a.pf = st.pfring.ptr;
+        a.pf_cap = st.pf_cap;
+        size_t wsz = size_t(B) * t.ndm_wt * t.nt_wt * t.nprofiles * st.N;
+        a.wt = st.wt.as<float>() + size_t(slot_wt) * wsz;
+        size_t osz = size_t(B) * t.ndm_out * t.nt_out;
+        a.out_max = st.out_max.as<char>() + size_t(slot_out) * osz * esize;
+        a.out_argmax = st.out_argmax.as<uint32_t>() + size_t(slot_out) * osz;
+        a.m_to_n = st.m_to_n.as<int>();
+        a.final_lag = st.final_lag.as<int>();
+        a.M = st.M; a.N = st.N; a.P = st.P; a.L = st.L;
+        a.ndm_out = int(t.ndm_out); a.nt_out = int(t.nt_out);
+        a.ndm_wt = int(t.ndm_wt); a.nt_wt = int(t.nt_wt);
+        a.Dout = st.Dout; a.Dcore = int(t.Dcore); a.tpad = st.tpad;
+        a.pf_shift = st.pf_shift;
+        a.s0 = ichunk * t.nt_ds;
+        a.beam0 = beam0;
+        launch_pf(a, dtype_code, int(B), s);
+    }
+    CUDA_CHECK(cudaEventRecord(ev_out_done[slot_out], s));
+    out_done_recorded[slot_out] = true;
+}
+
+GpuDedisperser::Outputs GpuDedisperser::acquire_output(long consumer_id, long seq_id, cudaStream_t stream, bool sync)
+{
+    return entry([&]() -> Outputs {
+        if (consumer_id < 0 || consumer_id >= params.num_consumers) throw runtime_error("GpuDedisperser::acquire_output(): bad consumer_id");
+        if (seq_id != next_acq_out[consumer_id])
+            throw runtime_error("GpuDedisperser::acquire_output(): expected seq_id=" + std::to_string(next_acq_out[consumer_id]) + ", got " + std::to_string(seq_id));
+        if (seq_id >= next_rel_in) throw runtime_error("GpuDedisperser::acquire_output(): seq_id has not been launched");
+        if (params.synchronous && next_rel_out[consumer_id] != seq_id)
+            throw runtime_error("GpuDedisperser::acquire_output(): synchronous consumer must release before acquiring the next batch");
+        if (seq_id - next_rel_out[consumer_id] >= nbatches_out)
+            throw runtime_error("GpuDedisperser::acquire_output(): too many unreleased output batches");
+        long slot = seq_id % nbatches_out;
+        if (sync) CUDA_CHECK(cudaEventSynchronize(ev_out_done[slot]));
+        else CUDA_CHECK(cudaStreamWaitEvent(stream, ev_out_done[slot], 0));
+        Outputs o;
+        o.dtype = plan.dtype;
+        o.nbeams = B;
+        o.ichunk_zero_based = seq_id / nbatches;
+        o.ichunk_fpga_based = o.ichunk_zero_based + params.initial_chunk;
+        o.ibeam = (seq_id % nbatches) * B;
+        for (long i = 0; i < plan.ntrees; i++) {
+            const DedispersionTree &t = plan.trees[i];
+            size_t osz = size_t(B) * t.ndm_out * t.nt_out;
+            o.ndm_out.push_back(t.ndm_out);
+            o.nt_out.push_back(t.nt_out);
+            o.out_max.push_back(s2[i].out_max.as<char>() + size_t(slot) * osz * esize);
+            o.out_argmax.push_back(s2[i].out_argmax.as<uint32_t>() + size_t(slot) * osz);
+        }
+        next_acq_out[consumer_id]++;
+        return o;
+    });
+}
+
+void GpuDedisperser::release_output(long consumer_id, long seq_id, cudaStream_t stream)
+{
+    entry([&]() {
+        if (consumer_id < 0 || consumer_id >= params.num_consumers) throw runtime_error("GpuDedisperser::release_output(): bad consumer_id");
+        if (seq_id != next_rel_out[consumer_id] || seq_id >= next_acq_out[consumer_id])
+            throw runtime_error("GpuDedisperser::release_output(): expected seq_id=" + std::to_string(next_rel_out[consumer_id]) + ", got " + std::to_string(seq_id));
+        long slot = seq_id % nbatches_out;
+        CUDA_CHECK(cudaEventRecord(ev_out_released[consumer_id][slot], stream));
+        out_released_recorded[consumer_id][slot] = true;
+        next_rel_out[consumer_id]++;
+    });
+}
+
+void GpuDedisperser::fill_all_weights(long itree, const float *host, long nelts)
+{
+    entry([&]() {
+        if (!allocated) throw runtime_error("GpuDedisperser::fill_all_weights(): allocate() was not called");
+        if (itree < 0 || itree >= plan.ntrees) throw runtime_error("GpuDedisperser::fill_all_weights(): itree out of range");
+        const DedispersionTree &t = plan.trees[itree];
+        long expect = nbatches_wt * B * t.ndm_wt * t.nt_wt * t.nprofiles * t.frequency_subbands.N;
+        if (nelts != expect)
+            throw runtime_error("GpuDedisperser::fill_all_weights(): expected " + std::to_string(expect) + " elements "
+                                "(nbatches_wt, beams_per_batch, ndm_wt, nt_wt, nprofiles, N), got " + std::to_string(nelts));
+        CUDA_CHECK(cudaMemcpyAsync(s2[itree].wt.ptr, host, nelts * sizeof(float), cudaMemcpyHostToDevice, compute));
+        CUDA_CHECK(cudaStreamSynchronize(compute));
+    });
+}
+
+}  // namespace pb2

@@ -1,0 +1,149 @@
+// dedisperser.hpp -- the B200 GpuDedisperser (host side).
+//
+// Mirrors pirate's GpuDedisperser (include/pirate/Dedisperser.hpp:45-254): sequential seq_id
+// cursors (seq_id = ichunk * nbatches + ibatch), acquire_input / release_input_and_launch_dd_kernels /
+// acquire_output / release_output with CUDA-event stream fencing, per-consumer output back-pressure,
+// and the "stoppable" error model (any failing entry point stops the object; later calls rethrow).
+//
+// Device memory layout (all allocated and zeroed by allocate()):
+//   inputs    nslots_in x (B, nfreq, nt_in)                     storage dtype
+//   tree0     (B, 2^rank, nt_in) level-0 tree                    storage dtype
+//   lds[p]    (total_beams, 2^(rank-1), cap_p) delay lines       storage dtype, cap_p = 2^k >= nt_p + 2^s1dd - 1
+//   ring[p]   per stage-1 output row (a, dm_brev): a delay line of capacity max_lag(row) + nt_p (rounded to 32)
+//   pfring[i] (total_beams, ndm_out, M, cap_i) subband rows       storage dtype, cap_i = 2^k >= nt + tpad + max subband lag
+//   hist      per-butterfly histories of the stage-1/stage-2 trees (fp32)
+//   outputs   nbatches_out x per-tree (B, ndm_out, nt_out) out_max (storage dtype) + out_argmax (uint32)
+//   weights   nbatches_wt x per-tree (B, ndm_wt, nt_wt, P, N) fp32
+
+#pragma once
+
+#include "kernels.cuh"
+#include "plan.hpp"
+
+#include <exception>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+namespace pb2 {
+
+struct TreeProgram
+{
+    std::vector<TreeOp> ops;
+    std::vector<int> phase_begin;
+    long hist_per_block = 0;
+    int nsteps = 0;
+    int nout = 0;
+};
+
+TreeProgram make_stage1_program(int dd_rank);
+TreeProgram make_stage2_program(int dd_rank, const FrequencySubbands &fs);
+
+struct DeviceBuffer
+{
+    void *ptr = nullptr;
+    size_t nbytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    DeviceBuffer(DeviceBuffer &&o) noexcept : ptr(o.ptr), nbytes(o.nbytes) { o.ptr = nullptr; o.nbytes = 0; }
+    ~DeviceBuffer();
+    void alloc(size_t n);   // cudaMalloc + cudaMemset(0)
+    void upload(const void *host, size_t n);
+    template<typename T> T *as() const { return (T *) ptr; }
+};
+
+class GpuDedisperser
+{
+public:
+    struct Params
+    {
+        int cuda_device_id = 0;
+        long nbatches_out = 0;      // 0 -> num_active_batches
+        long nbatches_wt = 0;       // 0 -> nbatches_out
+        long num_consumers = 1;
+        bool synchronous = true;
+        long initial_chunk = 0;
+    };
+
+    struct Outputs
+    {
+        Dtype dtype;
+        long nbeams = 0, ichunk_zero_based = 0, ichunk_fpga_based = 0, ibeam = 0;
+        std::vector<long> ndm_out, nt_out;
+        std::vector<void *> out_max;
+        std::vector<uint32_t *> out_argmax;
+    };
+
+    GpuDedisperser(const DedispersionPlan &plan, const Params &params);
+    ~GpuDedisperser();
+    GpuDedisperser(const GpuDedisperser &) = delete;
+    GpuDedisperser &operator=(const GpuDedisperser &) = delete;
+
+    void allocate();
+    void *acquire_input(long seq_id, cudaStream_t stream);
+    void release_input_and_launch_dd_kernels(long seq_id, cudaStream_t stream);
+    Outputs acquire_output(long consumer_id, long seq_id, cudaStream_t stream, bool sync);
+    void release_output(long consumer_id, long seq_id, cudaStream_t stream);
+    void fill_all_weights(long itree, const float *host, long nelts);
+    void stop(std::exception_ptr e = nullptr);
+
+    // Device bytes held by allocate() (for reporting).
+    size_t device_bytes() const { return total_bytes; }
+    // Number of kernels launched per (chunk, batch).
+    int kernels_per_batch() const;
+    // Bytes of HBM traffic per (chunk, batch) of each kernel class (algorithmic):
+    // [grid, lds, stage1, stage2, pf].
+    std::vector<double> algorithmic_bytes() const;
+
+    const DedispersionPlan plan;
+    const Params params;
+    long nbatches = 0, B = 0, total_beams = 0, nslots_in = 0, nbatches_out = 0, nbatches_wt = 0;
+
+private:
+    void check_alive() const;
+    template<typename F> auto entry(F &&f) -> decltype(f());
+    void launch_batch(long seq_id);
+
+    std::mutex mtx;
+    std::exception_ptr error;
+    bool stopped = false;
+    bool allocated = false;
+    long next_acq_in = 0, next_rel_in = 0;
+    std::vector<long> next_acq_out, next_rel_out;
+
+    int dtype_code = 0;
+    size_t esize = 4;
+    size_t total_bytes = 0;
+    cudaStream_t compute = nullptr;
+
+    // Per-slot events.
+    std::vector<cudaEvent_t> ev_in_acquired, ev_in_free, ev_out_done;
+    std::vector<std::vector<cudaEvent_t>> ev_out_released;   // [consumer][slot]
+    std::vector<bool> in_free_recorded, out_done_recorded;
+    std::vector<std::vector<bool>> out_released_recorded;
+
+    // Static device tables.
+    DeviceBuffer d_grid_f0, d_grid_cnt, d_grid_woff, d_grid_w;
+    struct Stage1
+    {
+        TreeProgram prog;
+        DeviceBuffer ops, phases, ring, ring_off, ring_cap, hist;
+        long ring_beam_stride = 0;
+        int nblocks = 0, nt = 0;
+        long lds_cap = 0;
+        DeviceBuffer lds;
+    };
+    struct Stage2
+    {
+        TreeProgram prog;
+        DeviceBuffer ops, phases, hist, pfring, m_to_n, final_lag, out_max, out_argmax, wt;
+        long pf_cap = 0;
+        int nblocks = 0, M = 0, N = 0, P = 0, L = 0, tpad = 0, pf_shift = 0, Dout = 0;
+    };
+    std::vector<Stage1> s1;
+    std::vector<Stage2> s2;
+    DeviceBuffer d_inputs, d_tree0, d_lds_state;
+};
+
+}  // namespace pb2

@@ -1,0 +1,89 @@
+"""Parity of the CUDA dedispersion path (through the public GpuDedisperser API, i.e. the C ABI)
+with the CPU oracle restating pirate's ReferenceDedisperser, on identical seeded inputs.
+
+float32 plans must match the fp32 oracle bit for bit (out_max) and token for token (out_argmax):
+the kernels perform the oracle's exact sequence of fp32 operations. float16/bfloat16 storage plans
+are compared with the FP64 oracle on the same (quantized) inputs, in units of the output sigma
+(bare unit-variance weights), and their tokens are checked by re-evaluating them in the oracle
+(ReferencePeakFindingKernel::eval_tokens, src_lib/PeakFindingKernel.cu:467)."""
+
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+# (rank, nfreq, nt, subbands, primary trees as (num_early_triggers, max_width), beams_per_gpu, beams_per_batch)
+FP32_CASES = [
+    (6, 100, 128, [1], [(0, 4)], 1, 1),
+    (8, 640, 256, [2, 2, 1], [(0, 16), (1, 8)], 2, 1),
+    (9, 300, 256, [1, 1, 1], [(1, 32), (0, 8), (1, 2)], 2, 2),
+    (10, 1024, 512, [0, 0, 1], [(0, 32), (0, 16), (0, 8)], 1, 1),
+    (11, 2000, 256, [3, 5, 3, 1], [(2, 8), (1, 4)], 4, 2),
+    (7, 50, 128, [1, 1], [(0, 1), (0, 2)], 3, 1),
+]
+
+
+def _cfg(case, dtype="float32"):
+    rank, nfreq, nt, sb, pts, bpg, bpb = case
+    prim = []
+    for ip, (net, w) in enumerate(pts):
+        prim.append(dict(num_early_triggers=net, max_width=w, dm_downsampling=0, time_downsampling=0,
+                         wt_dm_downsampling=2 ** ((rank - (1 if ip else 0) - net) // 2), wt_time_downsampling=16))
+    return H.toy_config(rank=rank, nfreq=nfreq, nt=nt, dtype=dtype, subbands=sb, beams_per_gpu=bpg,
+                        beams_per_batch=bpb, num_active_batches=1, primary_trees=prim)
+
+
+@pytest.mark.parametrize("case", FP32_CASES, ids=lambda c: "r%d_f%d_t%d" % (c[0], c[1], c[2]))
+def test_fp32_bitwise(pb2lib, case):
+    cfg = _cfg(case)
+    nb = cfg["beams_per_gpu"] // cfg["beams_per_batch"]
+    nchunks = 5
+    xs = H.make_inputs(cfg, nchunks, seed=case[0] * 7 + case[2])
+    orc, _ = H.run_oracle(cfg, xs[:0], [])  # shapes only
+    ws = H.make_weights(orc, seed=case[0], nbatches_wt=1)
+    _, ores = H.run_oracle(cfg, xs, ws, 1, 32)
+    plan, dd, gres = H.run_gpu(pb2lib, cfg, xs, ws)
+    for seq in range(nchunks * nb):
+        for i in range(orc.ntrees):
+            gm, ga = gres[seq][0][i], gres[seq][1][i]
+            om, oa = ores[seq][0][i], ores[seq][1][i]
+            assert gm.shape == om.shape
+            if not np.array_equal(gm, om):
+                d = np.abs(gm - om)
+                pytest.fail("seq %d tree %d: out_max differs at %d/%d entries, max |diff| %.3g" % (seq, i, (d > 0).sum(), d.size, d.max()))
+            if not np.array_equal(ga, oa):
+                pytest.fail("seq %d tree %d: out_argmax differs at %d/%d entries" % (seq, i, (ga != oa).sum(), ga.size))
+
+
+LOWP_CASES = [
+    ("float16", (8, 640, 256, [2, 2, 1], [(0, 16), (1, 8)], 2, 1), 1e-2),
+    ("bfloat16", (8, 640, 256, [2, 2, 1], [(0, 16), (1, 8)], 2, 1), 6e-2),
+    ("float16", (10, 1024, 512, [0, 0, 1], [(0, 32), (0, 16), (0, 8)], 1, 1), 1e-2),
+]
+
+
+@pytest.mark.parametrize("dtype,case,tol", LOWP_CASES, ids=lambda v: str(v) if isinstance(v, str) else None)
+def test_lowp_vs_fp64(pb2lib, dtype, case, tol):
+    """Max |error| of fp16/bf16-storage outputs against the FP64 oracle, in sigma, within 'tol'."""
+    cfg = _cfg(case, dtype)
+    nb = cfg["beams_per_gpu"] // cfg["beams_per_batch"]
+    nchunks = 4
+    xs = H.make_inputs(cfg, nchunks, seed=11)
+    orc64 = None
+    orc, _ = H.run_oracle(cfg, xs[:0], [], 1, 64)
+    ws = H.make_weights(orc, seed=3, kind="bare")
+    orc64, ores = H.run_oracle(cfg, xs, ws, 1, 64, keep=lambda o, s: None)
+    plan, dd, gres = H.run_gpu(pb2lib, cfg, xs, ws)
+    worst = 0.0
+    for seq in range(nchunks * nb):
+        for i in range(orc.ntrees):
+            gm, om = gres[seq][0][i], ores[seq][0][i]
+            worst = max(worst, float(np.abs(gm - om).max()))
+    assert worst <= tol, "max |gpu - fp64 oracle| = %.3g sigma > %.3g" % (worst, tol)
+    # Tokens: the trial each GPU token names must evaluate (in the oracle) to the oracle's max within tol.
+    last = len(xs) - 1
+    for i in range(orc.ntrees):
+        ev = orc64.eval_tokens(i, gres[last][1][i], ws[i][0])
+        assert np.abs(ev - ores[last][0][i]).max() <= 2 * tol
