@@ -1,0 +1,388 @@
+"""Benchmark of the B200 dedispersion path.
+
+Workload (a 'step' = one 2048-sample chunk of every beam): rank-16 tree (65536 tree channels) gridded
+from 16384 frequency channels over 400-800 MHz, 5 primary trees (time downsampling 1..16), peak
+finding up to width 32 per tree (64 samples in primary tree 1), full-band search (subband counts
+[0,0,0,0,1]), float16 storage with float32 arithmetic, 1 ms samples, seeded N(0,1) inputs.
+
+Metric: real-time beams per B200 = beams * chunk_seconds / seconds_per_chunk (pirate's definition,
+src_lib/GpuDedisperser.cpp:1598,1676). Prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--beams B] [--dtype float16] [--impl reference]
+
+Multi-GPU: the path shards by beam with no exchange step, so N GPUs run N independent replicas
+(one process per GPU under torchrun); value = all ranks' beams over the max-over-ranks time.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CHUNK = 2048
+SAMPLE_MS = 1.0
+CHUNK_SECONDS = CHUNK * SAMPLE_MS * 1e-3
+METRIC = "real-time beams/B200 (rank 16, fp16)"
+L2_BYTES = 126 * 2 ** 20
+
+
+def bench_config(beams, dtype):
+    prim = [dict(num_early_triggers=0, max_width=32, dm_downsampling=0, time_downsampling=0,
+                 wt_dm_downsampling=64, wt_time_downsampling=64) for _ in range(5)]
+    return dict(zone_nfreq=[16384], zone_freq_edges=[400.0, 800.0], time_sample_ms=SAMPLE_MS,
+                toplevel_tree_rank=16, time_samples_per_chunk=CHUNK, dtype=dtype,
+                frequency_subband_counts=[0, 0, 0, 0, 1], primary_trees=prim,
+                beams_per_gpu=beams, beams_per_batch=beams, num_active_batches=1,
+                future_write_max_samples=0, max_gpu_clag=10000)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    import pirate_b200 as pb
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cfg = bench_config(args.beams, args.dtype)
+    plan = pb.DedispersionPlan(pb.DedispersionConfig.from_dict(cfg))
+    dd = pb.GpuDedisperser(plan, cuda_device_id=dev, num_consumers=1)
+    dd.allocate()
+    tdt = getattr(torch, args.dtype)
+
+    # Unit-variance ("bare") peak-finding weights: out_max in sigma for N(0,1) input.
+    for i, t in enumerate(plan.trees):
+        var = [1.0]
+        for l in range((t.nprofiles - 1) // 3):
+            var += [2.0 ** (l + 1), 1.5 * 2.0 ** l, 2.5 * 2.0 ** l]
+        w = (1.0 / np.sqrt(np.array(var))).astype(np.float32)
+        arr = np.empty((dd.nbatches_wt, plan.beams_per_batch, t.ndm_wt, t.nt_wt, t.nprofiles, t.nsubbands), np.float32)
+        arr[...] = w[None, None, None, None, :, None]
+        dd.fill_all_weights(i, arr)
+
+    stream = torch.cuda.current_stream()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234 + rank)
+    seq = [0]
+
+    def step_device():
+        """One chunk of all beams; input stays resident in the (single) input slot."""
+        s = seq[0]
+        x = dd.acquire_input(s, stream)
+        if s == 0:
+            x.copy_(torch.randn(x.shape, generator=gen, device=x.device, dtype=torch.float32).to(tdt))
+        dd.release_input_and_launch_dd_kernels(s, stream)
+        dd.acquire_output(0, s, stream)
+        dd.release_output(0, s, stream)
+        seq[0] += 1
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+    dd.enable_timing(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step_device()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ktimes = dd.kernel_times()
+    dd.enable_timing(False)
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    ms_per_step = ms / args.steps
+
+    # End to end through the public API: pinned host input -> H2D into the acquired input buffer,
+    # kernels, D2H of every tree's out_max and out_argmax, per step.
+    xin = torch.empty(dd.acquire_input(seq[0], stream).shape, dtype=tdt, pin_memory=True)
+    xin.copy_(torch.randn(xin.shape, dtype=torch.float32).to(tdt))
+    dd.release_input_and_launch_dd_kernels(seq[0], stream)
+    dd.acquire_output(0, seq[0], stream)
+    dd.release_output(0, seq[0], stream)
+    seq[0] += 1
+    outs_host = None
+    h2d = xin.numel() * xin.element_size()
+    d2h = 0
+    for t in plan.trees:
+        d2h += plan.beams_per_batch * t.ndm_out * t.nt_out * (xin.element_size() + 4)
+
+    def step_e2e():
+        nonlocal outs_host
+        s = seq[0]
+        x = dd.acquire_input(s, stream)
+        x.copy_(xin, non_blocking=True)
+        dd.release_input_and_launch_dd_kernels(s, stream)
+        o = dd.acquire_output(0, s, stream)
+        if outs_host is None:
+            outs_host = [(torch.empty(m.shape, dtype=m.dtype, pin_memory=True),
+                          torch.empty(a.shape, dtype=a.dtype, pin_memory=True)) for m, a in zip(o.out_max, o.out_argmax)]
+        for (hm, ha), m, a in zip(outs_host, o.out_max, o.out_argmax):
+            hm.copy_(m, non_blocking=True)
+            ha.copy_(a, non_blocking=True)
+        dd.release_output(0, s, stream)
+        seq[0] += 1
+
+    e2e_steps = max(2, min(args.steps, 8))
+    for _ in range(2):
+        step_e2e()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        step_e2e()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ems = f0.elapsed_time(f1)
+    if world > 1:
+        t = torch.tensor([ems], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ems = float(t.item())
+
+    alg = dd.algorithmic_bytes()
+    return dict(plan=plan, dd=dd, ms_per_step=ms_per_step, e2e_ms_per_step=ems / e2e_steps, ktimes=ktimes,
+                alg=alg, clocks=clk.summary(), h2d=h2d, d2h=d2h, device_bytes=dd.device_bytes(),
+                kernels_per_batch=dd.kernels_per_batch())
+
+
+def cpu_sample(nchunks=1, dtype="float16"):
+    """Times the CPU oracle (fp32 restatement of pirate's ReferenceDedisperser, sophistication 1)
+    on one beam of the bench workload; returns seconds per chunk."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    cfg = bench_config(1, "float32")
+    cfg["dtype"] = dtype if dtype != "bfloat16" else "float16"   # same plan shapes as the GPU run
+    orc = oracle.OracleDedisperser(cfg, 1, 32)
+    ws = [oracle.bare_weights(orc.wt_shape(i), orc.trees[i]["nprofiles"]) for i in range(orc.ntrees)]
+    x = np.random.default_rng(0).standard_normal((1, 16384, CHUNK)).astype(np.float32)
+    t0 = time.time()
+    for _ in range(nchunks):
+        orc.dedisperse(0, x, ws)
+    return (time.time() - t0) / nchunks
+
+
+def _cpu_worker(q, nchunks, dtype):
+    q.put(cpu_sample(nchunks, dtype))
+
+
+def run_reference(args, rank, world):
+    """The reference arm: pirate's CPU dedisperser (restated by the oracle; pirate itself needs ksgpu,
+    yaml-cpp and MKL, which are not installed) on the host cores, one beam per process."""
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+    ncores = os.cpu_count() or 1
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except Exception:
+        avail = 64 << 30
+    nproc = int(max(1, min(ncores, avail // (24 << 30))))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    t0 = time.time()
+    ps = [ctx.Process(target=_cpu_worker, args=(q, 1, args.dtype)) for _ in range(nproc)]
+    for p in ps:
+        p.start()
+    per = [q.get() for _ in ps]
+    for p in ps:
+        p.join()
+    wall = time.time() - t0
+    sec = max(per)
+    value = nproc * CHUNK_SECONDS / sec
+    return dict(value=value, sec=sec, nproc=nproc, wall=wall)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--beams", type=int, default=4)
+    ap.add_argument("--dtype", default="float16", choices=["float16", "bfloat16", "float32"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    cfg_json = {"workload": "rank-16 tree, 16384 channels 400-800 MHz, 5 primary trees (time downsampling 1-16), "
+                            "2048-sample chunks, widths to 32 per tree, full-band search",
+                "beams_per_gpu": args.beams, "chunk_samples": CHUNK, "sample_ms": SAMPLE_MS,
+                "storage": args.dtype, "parallelism": "replicas x%d (beams shard, no collective)" % args.gpus,
+                "l2": "inputs and lag state exceed L2 (126 MB) every step"}
+
+    if args.impl == "reference":
+        if world > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo")
+        r = run_reference(args, rank, world)
+        if rank == 0:
+            line = {"metric": METRIC, "value": r["value"], "unit": "beams", "impl": "reference", "n_gpus": args.gpus,
+                    "steps": 1, "warmup": 0, "ms_per_step": r["sec"] * 1e3, "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1)",
+                    "config": cfg_json,
+                    "cpu_baseline": {"value": r["value"], "unit": "beams", "cores": r["nproc"], "kind": "port",
+                                     "sample": "1 chunk of 1 beam per process, %d processes (fp32 oracle restating "
+                                               "ReferenceDedisperser sophistication 1)" % r["nproc"]},
+                    "e2e": {"value": r["value"], "unit": "beams", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    r = run_ours(args, rank, world)
+    peak, peak_kind = load_peaks()
+    nbeams_total = args.beams * world
+    value = nbeams_total * CHUNK_SECONDS / (r["ms_per_step"] * 1e-3)
+    e2e = nbeams_total * CHUNK_SECONDS / (r["e2e_ms_per_step"] * 1e-3)
+
+    classes = ["grid", "lds", "stage1", "stage2", "pf"]
+    kt = r["ktimes"]
+    tot_ms = sum(kt[c][0] for c in classes)
+    dom = max(classes, key=lambda c: kt[c][0])
+    nsteps = args.steps
+    dom_ms_per_step = kt[dom][0] / nsteps
+    dom_launches_per_step = kt[dom][1] / nsteps
+    dom_bytes = r["alg"][classes.index(dom)]
+    achieved = dom_bytes / (dom_ms_per_step * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                tj = json.load(f)
+            if dom in tj and tj[dom].get("bytes_per_beam_chunk"):
+                traffic = tj[dom]["bytes_per_beam_chunk"] * args.beams
+        except Exception:
+            traffic = None
+    alg_total = sum(r["alg"])
+    e2e_alg_gbs = alg_total / (r["ms_per_step"] * 1e-3) / 1e9
+
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 2), "unit": "beams", "n_gpus": world, "steps": nsteps,
+                "warmup": args.warmup, "ms_per_step": round(r["ms_per_step"], 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1), seeded",
+                "config": cfg_json,
+                "e2e": {"value": round(e2e, 2), "unit": "beams", "h2d_bytes_per_step": int(r["h2d"]),
+                        "d2h_bytes_per_step": int(r["d2h"]), "ms_per_step": round(r["e2e_ms_per_step"], 4)},
+                "gpu_launches": int(r["kernels_per_batch"] * nsteps),
+                "roofline": {"bound": "hbm", "kernel": dom, "launches_per_step": dom_launches_per_step,
+                             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                             "traffic": traffic, "algorithmic_bytes_per_step": dom_bytes},
+                "kernels": {c: {"ms_per_step": round(kt[c][0] / nsteps, 4), "share": round(kt[c][0] / tot_ms, 4) if tot_ms else None,
+                                "alg_GBps": round(r["alg"][i] / (kt[c][0] / nsteps * 1e-3) / 1e9, 1) if kt[c][0] else None}
+                            for i, c in enumerate(classes)},
+                "pipeline_alg_GBps": round(e2e_alg_gbs, 1),
+                "device_bytes": r["device_bytes"],
+                "clocks": r["clocks"]}
+        if not args.no_cpu_baseline and world == 1:
+            sec = cpu_sample(1, args.dtype)
+            line["cpu_baseline"] = {"value": round(CHUNK_SECONDS / sec, 4), "unit": "beams", "cores": 1, "kind": "port",
+                                    "sample": "1 chunk of 1 beam (fp32 oracle restating ReferenceDedisperser, "
+                                              "sophistication 1), %.1f s" % sec}
+        print(json.dumps(line), flush=True)
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -85,6 +85,8 @@ def lib():
         "pb2_dd_stop": (ctypes.c_int, [vp]),
         "pb2_dd_kernels_per_batch": (ctypes.c_int, [vp, lp]),
         "pb2_dd_algorithmic_bytes": (ctypes.c_int, [vp, dp]),
+        "pb2_dd_enable_timing": (ctypes.c_int, [vp, ctypes.c_int]),
+        "pb2_dd_kernel_times": (ctypes.c_int, [vp, dp, lp]),
         "pb2_dd_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
@@ -334,6 +336,18 @@ class GpuDedisperser:
         out = (ctypes.c_double * 5)()
         _check(lib().pb2_dd_algorithmic_bytes(self._h, out))
         return list(out)
+
+    KERNEL_CLASSES = ("grid", "lds", "stage1", "stage2", "pf")
+
+    def enable_timing(self, on=True):
+        _check(lib().pb2_dd_enable_timing(self._h, 1 if on else 0))
+
+    def kernel_times(self):
+        """{class: (milliseconds, launches)} accumulated since enable_timing()."""
+        ms = (ctypes.c_double * 5)()
+        n = (ctypes.c_long * 5)()
+        _check(lib().pb2_dd_kernel_times(self._h, ms, n))
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
 
     def acquire_input(self, seq_id, stream=None):
         ptr = ctypes.c_void_p()

@@ -267,6 +267,16 @@ int pb2_dd_algorithmic_bytes(const pb2_dedisperser *dd, double *out5)
     });
 }
 
+int pb2_dd_enable_timing(pb2_dedisperser *dd, int on)
+{
+    return guard([&] { REQUIRE_PTR(dd); dd->d->enable_timing(on != 0); });
+}
+
+int pb2_dd_kernel_times(pb2_dedisperser *dd, double *ms5, long *counts5)
+{
+    return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(ms5); REQUIRE_PTR(counts5); dd->d->kernel_times(ms5, counts5); });
+}
+
 void pb2_dd_destroy(pb2_dedisperser *dd) { delete dd; }
 
 }  // extern "C"

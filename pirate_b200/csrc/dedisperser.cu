@@ -39,145 +39,6 @@ void DeviceBuffer::upload(const void *host, size_t n)
 
 
 // -------------------------------------------------------------------------------------------------
-// Tree programs.
-//
-// Stage 1 (src_lib/ReferenceTree.cpp:120-300 with no subbands): step r pairs rows i and i + 2^r
-// (i = fo * 2^(r+1) + j, j < 2^r) with lag bit_reverse(j, r).
-//
-// Stage 2 follows ReferenceTree::dedisperse_2d (src_lib/ReferenceTree.cpp:120-300) step by step:
-// pf-level-0 subbands are copies of the current rows; staggered subbands at pf_level > 0 are
-// butterflies over band pairs (pfs, pfs+1) whose even members coincide with in-place butterflies.
-
-
-static TreeOp make_bfly(int row0, int row1, int lag, int kind, long &hoff)
-{
-    TreeOp op;
-    op.row0 = int16_t(row0);
-    op.row1 = int16_t(row1);
-    op.kind = int16_t(kind);
-    op.pad = 0;
-    op.lag = lag;
-    long cap = next_pow2(lag + 1);
-    op.hist_off = int32_t(hoff);
-    op.hist_mask = int32_t(cap - 1);
-    hoff += cap;
-    op.out0 = op.out1 = -1;
-    return op;
-}
-
-TreeProgram make_stage1_program(int R)
-{
-    TreeProgram P;
-    long hoff = 0;
-    for (int r = 0; r < R; r++) {
-        P.phase_begin.push_back(P.ops.size());
-        int ndm_in = 1 << r;
-        for (int fo = 0; fo < (1 << (R - r - 1)); fo++)
-            for (int j = 0; j < ndm_in; j++) {
-                int row0 = fo * 2 * ndm_in + j;
-                P.ops.push_back(make_bfly(row0, row0 + ndm_in, bit_reverse(j, r), 0, hoff));
-            }
-    }
-    P.phase_begin.push_back(P.ops.size());
-    P.hist_per_block = hoff;
-    P.nsteps = R;
-    P.nout = 0;
-    return P;
-}
-
-TreeProgram make_stage2_program(int R, const FrequencySubbands &fs)
-{
-    TreeProgram P;
-    const int pf_rank = fs.pf_rank, M = fs.M, pf_ndm = 1 << (R - pf_rank);
-    if (pf_rank > R) throw runtime_error("make_stage2_program: pf_rank > dd_rank");
-    long hoff = 0;
-    int mcurr = 0;
-
-    for (int r = 0; r <= R; r++) {
-        int ndm_in = 1 << r;
-        vector<TreeOp> copies, stag, tree;
-
-        if (r == R - pf_rank) {
-            int pf_ns = fs.subband_counts[0];
-            for (int dm_in = 0; dm_in < ndm_in; dm_in++) {
-                int dbr = bit_reverse(dm_in, r);
-                for (int pfs = 0; pfs < pf_ns; pfs++) {
-                    TreeOp op;
-                    memset(&op, 0, sizeof(op));
-                    op.kind = 2;
-                    op.row0 = int16_t(pfs * ndm_in + dbr);
-                    op.row1 = op.row0;
-                    op.out0 = dm_in * M + mcurr + pfs;
-                    op.out1 = -1;
-                    copies.push_back(op);
-                }
-            }
-            mcurr += pf_ns;
-        }
-
-        if (r < R) {
-            for (int fo = 0; fo < (1 << (R - r - 1)); fo++)
-                for (int j = 0; j < ndm_in; j++) {
-                    int row0 = fo * 2 * ndm_in + j;
-                    tree.push_back(make_bfly(row0, row0 + ndm_in, bit_reverse(j, r), 0, hoff));
-                }
-            int pf_level = r + pf_rank - R + 1;
-            if (pf_level > 0) {
-                int pf_ns = fs.subband_counts[pf_level], pf_nd2 = 1 << (pf_level - 1);
-                if (ndm_in != pf_ndm * pf_nd2) throw runtime_error("make_stage2_program: inconsistent subband shape");
-                for (int pf_dm = 0; pf_dm < pf_ndm; pf_dm++)
-                    for (int d2 = 0; d2 < pf_nd2; d2++) {
-                        int dm_in = pf_dm * pf_nd2 + d2;
-                        int dbr = bit_reverse(dm_in, r);
-                        for (int pfs = 0; pfs < pf_ns; pfs++) {
-                            int m = mcurr + pfs * 2 * pf_nd2 + 2 * d2;
-                            int o0 = pf_dm * M + m;
-                            if ((pfs & 1) == 0) {
-                                TreeOp &op = tree.at((pfs / 2) * ndm_in + dbr);
-                                if (op.lag != dm_in || op.row0 != pfs * ndm_in + dbr) throw runtime_error("make_stage2_program: pairing mismatch");
-                                op.out0 = o0;
-                                op.out1 = o0 + 1;
-                            }
-                            else {
-                                int row0 = pfs * ndm_in + dbr;
-                                TreeOp op = make_bfly(row0, row0 + ndm_in, dm_in, 1, hoff);
-                                op.out0 = o0;
-                                op.out1 = o0 + 1;
-                                stag.push_back(op);
-                            }
-                        }
-                    }
-                mcurr += pf_ns * 2 * pf_nd2;
-            }
-        }
-
-        if (r < R || !copies.empty()) {
-            P.phase_begin.push_back(P.ops.size());
-            P.ops.insert(P.ops.end(), copies.begin(), copies.end());
-            P.ops.insert(P.ops.end(), stag.begin(), stag.end());
-            P.ops.insert(P.ops.end(), tree.begin(), tree.end());
-        }
-    }
-    P.phase_begin.push_back(P.ops.size());
-    if (mcurr != M) throw runtime_error("make_stage2_program: multiplet count mismatch");
-
-    // Every subband output row must be produced exactly once per tile.
-    P.nout = pf_ndm * M;
-    vector<int> seen(P.nout, 0);
-    for (const TreeOp &op : P.ops) {
-        if (op.out0 >= 0) seen.at(op.out0)++;
-        if (op.out1 >= 0) seen.at(op.out1)++;
-    }
-    for (int c : seen)
-        if (c != 1) throw runtime_error("make_stage2_program: subband outputs not covered exactly once");
-
-    P.hist_per_block = hoff;
-    P.nsteps = R;
-    return P;
-}
-
-
-// -------------------------------------------------------------------------------------------------
 // GpuDedisperser
 
 
@@ -204,6 +65,8 @@ GpuDedisperser::~GpuDedisperser()
     cudaGetDevice(&dev);
     cudaSetDevice(params.cuda_device_id);
     if (compute) cudaStreamSynchronize(compute);
+    for (auto &v : tev) for (auto &pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     auto kill = [](vector<cudaEvent_t> &v) { for (cudaEvent_t e : v) if (e) cudaEventDestroy(e); v.clear(); };
     kill(ev_in_acquired);
     kill(ev_in_free);
@@ -270,6 +133,55 @@ std::vector<double> GpuDedisperser::algorithmic_bytes() const
     return {grid, lds, st1, st2, pf};
 }
 
+void GpuDedisperser::enable_timing(bool on)
+{
+    entry([&]() {
+        timing = on;
+        tev.assign(5, {});
+        for (int i = 0; i < 5; i++) { tms[i] = 0; tcount[i] = 0; }
+    });
+}
+
+// Records an event on the compute stream. With start == nullptr returns a fresh start event;
+// otherwise closes the interval (start, now) for class 'cls'.
+cudaEvent_t GpuDedisperser::tick(int cls, cudaEvent_t start)
+{
+    if (!timing) return nullptr;
+    cudaEvent_t e;
+    if (!ev_pool.empty()) { e = ev_pool.back(); ev_pool.pop_back(); }
+    else CUDA_CHECK(cudaEventCreate(&e));
+    CUDA_CHECK(cudaEventRecord(e, compute));
+    if (start) {
+        tev[cls].push_back({start, e});
+        if (tev[cls].size() > 256) drain_timing();
+    }
+    return e;
+}
+
+void GpuDedisperser::drain_timing()
+{
+    for (int c = 0; c < 5; c++) {
+        for (auto &pr : tev[c]) {
+            CUDA_CHECK(cudaEventSynchronize(pr.second));
+            float ms = 0;
+            CUDA_CHECK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            tms[c] += ms;
+            tcount[c]++;
+            ev_pool.push_back(pr.first);
+            ev_pool.push_back(pr.second);
+        }
+        tev[c].clear();
+    }
+}
+
+void GpuDedisperser::kernel_times(double *ms5, long *counts5)
+{
+    entry([&]() {
+        if (timing) drain_timing();
+        for (int i = 0; i < 5; i++) { ms5[i] = tms[i]; counts5[i] = tcount[i]; }
+    });
+}
+
 void GpuDedisperser::allocate()
 {
     entry([&]() {
@@ -324,12 +236,12 @@ void GpuDedisperser::allocate()
         for (long p = 0; p < npri; p++) {
             Stage1 &st = s1[p];
             int R1 = plan.stage1_dd_rank[p], A1 = plan.stage1_amb_rank[p];
-            st.prog = make_stage1_program(R1);
+            if (R1 < 1 || R1 > 8) throw runtime_error("GpuDedisperser: stage-1 dd rank must be in [1, 8]");
+            st.rank = R1;
             st.nblocks = 1 << A1;
             st.nt = int(nt >> p);
-            st.ops.upload(st.prog.ops.data(), st.prog.ops.size() * sizeof(TreeOp));
-            st.phases.upload(st.prog.phase_begin.data(), st.prog.phase_begin.size() * sizeof(int));
-            add(st.hist, size_t(total_beams) * st.nblocks * st.prog.hist_per_block * sizeof(float));
+            st.state_per_block = stage1_state_floats(R1);
+            add(st.state, size_t(total_beams) * st.nblocks * st.state_per_block * sizeof(float));
 
             long nrows = pow2(R1 + A1);
             vector<long> off(nrows);
@@ -357,33 +269,31 @@ void GpuDedisperser::allocate()
             const DedispersionTree &t = plan.trees[i];
             Stage2 &st = s2[i];
             const FrequencySubbands &fs = t.frequency_subbands;
-            st.prog = make_stage2_program(t.dd_rank, fs);
+            if (t.dd_rank < 1 || t.dd_rank > 8) throw runtime_error("GpuDedisperser: stage-2 dd rank must be in [1, 8]");
+            if (fs.pf_rank != split_rb(t.dd_rank)) throw runtime_error("GpuDedisperser: unexpected peak-finding rank");
             st.nblocks = 1 << t.amb_rank;
             st.M = fs.M;
             st.N = fs.N;
             st.P = t.nprofiles;
             st.L = std::max(integer_log2(t.pf.max_width), 1);
             st.tpad = int(std::max(2 * t.pf.max_width, 4L));
-            st.pf_shift = t.dd_rank - fs.pf_rank;
             st.Dout = int(t.pf.time_downsampling);
-            st.ops.upload(st.prog.ops.data(), st.prog.ops.size() * sizeof(TreeOp));
-            st.phases.upload(st.prog.phase_begin.data(), st.prog.phase_begin.size() * sizeof(int));
-            add(st.hist, size_t(total_beams) * st.nblocks * st.prog.hist_per_block * sizeof(float));
+            st.state_per_block = stage2_state_floats(t.dd_rank);
+            add(st.state, size_t(total_beams) * st.nblocks * st.state_per_block * sizeof(float));
+            int mb = 0;
+            for (int l = 0; l <= fs.pf_rank; l++) {
+                st.sb_count[l] = int(fs.subband_counts[l]);
+                st.sb_mbase[l] = mb;
+                mb += int(fs.subband_counts[l]) << l;
+            }
+            if (mb != st.M) throw runtime_error("GpuDedisperser: multiplet count mismatch");
 
-            // Subband alignment lag of (pf_dm, m): (2^pf_rank - fhi(m)) * pf_dm (src_lib/ReferenceTree.cpp:41-50).
-            int npfdm = 1 << st.pf_shift;
-            vector<int> fl(npfdm * st.M), m2n(st.M);
-            long maxlag = 0;
-            for (int d = 0; d < npfdm; d++)
-                for (int m = 0; m < st.M; m++) {
-                    long lag = (pow2(fs.pf_rank) - fs.m_to_fhi(m)) * d;
-                    fl[d * st.M + m] = int(lag);
-                    maxlag = std::max(maxlag, lag);
-                }
+            // The stage-2 kernel emits subband rows already delayed by their alignment lag
+            // (see regtree.cuh), so the peak finder reads every row at the same time.
+            vector<int> m2n(st.M);
             for (int m = 0; m < st.M; m++) m2n[m] = int(fs.m_to_n[m]);
-            st.final_lag.upload(fl.data(), fl.size() * sizeof(int));
             st.m_to_n.upload(m2n.data(), m2n.size() * sizeof(int));
-            st.pf_cap = next_pow2(t.nt_ds + st.tpad + maxlag + st.Dout);
+            st.pf_cap = next_pow2(t.nt_ds + st.tpad + st.Dout);
             add(st.pfring, size_t(total_beams) * t.ndm_out * st.M * st.pf_cap * esize);
             add(st.out_max, size_t(nbatches_out) * B * t.ndm_out * t.nt_out * esize);
             add(st.out_argmax, size_t(nbatches_out) * B * t.ndm_out * t.nt_out * sizeof(uint32_t));
@@ -438,7 +348,9 @@ void GpuDedisperser::launch_batch(long seq_id)
     g.chan_woff = d_grid_woff.as<int>();
     g.chan_w = d_grid_w.as<float>();
     g.F = int(F); g.N = int(N); g.T = int(nt);
+    cudaEvent_t t0 = tick(0, nullptr);
     launch_grid(g, dtype_code, int(B), s);
+    tick(0, t0);
     CUDA_CHECK(cudaEventRecord(ev_in_free[slot_in], s));
     in_free_recorded[slot_in] = true;
 
@@ -454,19 +366,18 @@ void GpuDedisperser::launch_batch(long seq_id)
         l.state = d_lds_state.as<float>();
         l.ichunk = ichunk;
         l.beam0 = beam0; l.B = int(B); l.total_beams = int(total_beams);
+        cudaEvent_t t1 = tick(1, nullptr);
         launch_lds(l, dtype_code, s);
+        tick(1, t1);
     }
 
     for (long p = 0; p < npri; p++) {
         Stage1 &st = s1[p];
         Stage1Args a;
         memset(&a, 0, sizeof(a));
-        a.ops = st.ops.as<TreeOp>();
-        a.phase_begin = st.phases.as<int>();
-        a.nphases = int(st.prog.phase_begin.size() - 1);
-        a.nrows = 1 << plan.stage1_dd_rank[p];
-        a.hist_per_block = st.prog.hist_per_block;
-        a.hist = st.hist.as<float>();
+        a.rank = st.rank;
+        a.state_per_block = st.state_per_block;
+        a.state = st.state.as<float>();
         if (p == 0) {
             a.in = d_tree0.ptr;
             a.in_beam_stride = N * nt;
@@ -492,7 +403,9 @@ void GpuDedisperser::launch_batch(long seq_id)
         a.s0 = ichunk * st.nt;
         a.nt = st.nt;
         a.beam0 = beam0;
+        cudaEvent_t t2 = tick(2, nullptr);
         launch_stage1(a, dtype_code, st.nblocks, int(B), s);
+        tick(2, t2);
     }
 
     for (long i = 0; i < plan.ntrees; i++) {
@@ -501,28 +414,26 @@ void GpuDedisperser::launch_batch(long seq_id)
         Stage1 &src = s1[t.primary_tree_index];
         Stage2Args a;
         memset(&a, 0, sizeof(a));
-        a.ops = st.ops.as<TreeOp>();
-        a.phase_begin = st.phases.as<int>();
-        a.nphases = int(st.prog.phase_begin.size() - 1);
-        a.nrows = 1 << t.dd_rank;
-        a.hist_per_block = st.prog.hist_per_block;
-        a.hist = st.hist.as<float>();
+        a.rank = t.dd_rank;
+        a.state_per_block = st.state_per_block;
+        a.state = st.state.as<float>();
         a.ring = src.ring.ptr;
         a.ring_off = src.ring_off.as<long>();
         a.ring_cap = src.ring_cap.as<int>();
         a.ring_beam_stride = src.ring_beam_stride;
         a.amb_rank = t.amb_rank;
-        a.dd_rank = t.dd_rank;
         a.uflag = (t.primary_tree_index > 0) ? 1 : 0;
+        for (int l = 0; l < 5; l++) { a.sb_count[l] = st.sb_count[l]; a.sb_mbase[l] = st.sb_mbase[l]; }
         a.pf = st.pfring.ptr;
         a.M = st.M;
         a.ndm_out = int(t.ndm_out);
-        a.pf_shift = st.pf_shift;
         a.pf_cap = st.pf_cap;
         a.s0 = ichunk * t.nt_ds;
         a.nt = t.nt_ds;
         a.beam0 = beam0;
+        cudaEvent_t t3 = tick(3, nullptr);
         launch_stage2(a, dtype_code, st.nblocks, int(B), s);
+        tick(3, t3);
     }
 
     // Output back-pressure: slot_out is reusable once every consumer released seq_id - nbatches_out.
@@ -543,15 +454,15 @@ void GpuDedisperser::launch_batch(long seq_id)
         a.out_max = st.out_max.as<char>() + size_t(slot_out) * osz * esize;
         a.out_argmax = st.out_argmax.as<uint32_t>() + size_t(slot_out) * osz;
         a.m_to_n = st.m_to_n.as<int>();
-        a.final_lag = st.final_lag.as<int>();
         a.M = st.M; a.N = st.N; a.P = st.P; a.L = st.L;
         a.ndm_out = int(t.ndm_out); a.nt_out = int(t.nt_out);
         a.ndm_wt = int(t.ndm_wt); a.nt_wt = int(t.nt_wt);
         a.Dout = st.Dout; a.Dcore = int(t.Dcore); a.tpad = st.tpad;
-        a.pf_shift = st.pf_shift;
         a.s0 = ichunk * t.nt_ds;
         a.beam0 = beam0;
+        cudaEvent_t t4 = tick(4, nullptr);
         launch_pf(a, dtype_code, int(B), s);
+        tick(4, t4);
     }
     CUDA_CHECK(cudaEventRecord(ev_out_done[slot_out], s));
     out_done_recorded[slot_out] = true;

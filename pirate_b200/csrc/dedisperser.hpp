@@ -11,7 +11,7 @@
 //   lds[p]    (total_beams, 2^(rank-1), cap_p) delay lines       storage dtype, cap_p = 2^k >= nt_p + 2^s1dd - 1
 //   ring[p]   per stage-1 output row (a, dm_brev): a delay line of capacity max_lag(row) + nt_p (rounded to 32)
 //   pfring[i] (total_beams, ndm_out, M, cap_i) subband rows       storage dtype, cap_i = 2^k >= nt + tpad + max subband lag
-//   hist      per-butterfly histories of the stage-1/stage-2 trees (fp32)
+//   state     per-block tree state of the stage-1/stage-2 kernels (fp32): phase delay line + histories
 //   outputs   nbatches_out x per-tree (B, ndm_out, nt_out) out_max (storage dtype) + out_argmax (uint32)
 //   weights   nbatches_wt x per-tree (B, ndm_wt, nt_wt, P, N) fp32
 
@@ -26,18 +26,6 @@
 #include <vector>
 
 namespace pb2 {
-
-struct TreeProgram
-{
-    std::vector<TreeOp> ops;
-    std::vector<int> phase_begin;
-    long hist_per_block = 0;
-    int nsteps = 0;
-    int nout = 0;
-};
-
-TreeProgram make_stage1_program(int dd_rank);
-TreeProgram make_stage2_program(int dd_rank, const FrequencySubbands &fs);
 
 struct DeviceBuffer
 {
@@ -96,6 +84,12 @@ public:
     // [grid, lds, stage1, stage2, pf].
     std::vector<double> algorithmic_bytes() const;
 
+    // Kernel timing: when enabled, CUDA events bracket each kernel class
+    // [grid, lds, stage1, stage2, pf] on the compute stream; kernel_times() synchronizes and returns
+    // the accumulated milliseconds and launch counts since the last reset.
+    void enable_timing(bool on);
+    void kernel_times(double *ms5, long *counts5);
+
     const DedispersionPlan plan;
     const Params params;
     long nbatches = 0, B = 0, total_beams = 0, nslots_in = 0, nbatches_out = 0, nbatches_wt = 0;
@@ -127,20 +121,27 @@ private:
     DeviceBuffer d_grid_f0, d_grid_cnt, d_grid_woff, d_grid_w;
     struct Stage1
     {
-        TreeProgram prog;
-        DeviceBuffer ops, phases, ring, ring_off, ring_cap, hist;
-        long ring_beam_stride = 0;
-        int nblocks = 0, nt = 0;
+        DeviceBuffer ring, ring_off, ring_cap, state;
+        long ring_beam_stride = 0, state_per_block = 0;
+        int nblocks = 0, nt = 0, rank = 0;
         long lds_cap = 0;
         DeviceBuffer lds;
     };
     struct Stage2
     {
-        TreeProgram prog;
-        DeviceBuffer ops, phases, hist, pfring, m_to_n, final_lag, out_max, out_argmax, wt;
-        long pf_cap = 0;
-        int nblocks = 0, M = 0, N = 0, P = 0, L = 0, tpad = 0, pf_shift = 0, Dout = 0;
+        DeviceBuffer state, pfring, m_to_n, out_max, out_argmax, wt;
+        long pf_cap = 0, state_per_block = 0;
+        int nblocks = 0, M = 0, N = 0, P = 0, L = 0, tpad = 0, Dout = 0;
+        int sb_count[5] = {0, 0, 0, 0, 0}, sb_mbase[5] = {0, 0, 0, 0, 0};
     };
+    bool timing = false;
+    std::vector<std::vector<std::pair<cudaEvent_t, cudaEvent_t>>> tev;   // per class, pending event pairs
+    double tms[5] = {0, 0, 0, 0, 0};
+    long tcount[5] = {0, 0, 0, 0, 0};
+    std::vector<cudaEvent_t> ev_pool;
+    cudaEvent_t tick(int cls, cudaEvent_t start);
+    void drain_timing();
+
     std::vector<Stage1> s1;
     std::vector<Stage2> s2;
     DeviceBuffer d_inputs, d_tree0, d_lds_state;

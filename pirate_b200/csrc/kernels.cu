@@ -175,181 +175,419 @@ __global__ void __launch_bounds__(128) lds_kernel(LdsArgs a)
 
 
 // -------------------------------------------------------------------------------------------------
-// Tree programs (see TreeOp in kernels.cuh). 'cur' holds the tile (nrows x kTreeTile) at the start
-// of each phase; butterflies write the next state into 'nxt'. Returns the buffer holding the result.
+// Two-phase register trees (see regtree.cuh). Lane = time sample within a 32-sample tile.
 
 
-template<typename OutF>
-__device__ __forceinline__ float *run_program(float *cur, float *nxt, const TreeOp *__restrict__ ops,
-                                              const int *__restrict__ phase_begin, int nphases, int nsteps,
-                                              float *__restrict__ hist, long s_tile, OutF out)
+constexpr unsigned kFull = 0xffffffffu;
+
+// Row 'x' of the current tile lagged by L (< 32) samples, with 'p' = the same row in the previous
+// tile: the lane that holds the wanted sample offers x or p, and one shuffle delivers it.
+__device__ __forceinline__ float lagged(float x, float p, int L, int lane)
 {
-    constexpr int TT = kTreeTile;
-    const int tid = threadIdx.x, nthr = blockDim.x;
-
-    for (int ph = 0; ph < nphases; ph++) {
-        int ob = phase_begin[ph], oe = phase_begin[ph + 1];
-        int nitems = (oe - ob) * TT;
-
-        for (int it = tid; it < nitems; it += nthr) {
-            const TreeOp op = ops[ob + it / TT];
-            int t = it % TT;
-            if (op.kind == 2) {
-                out(op.out0, t, cur[op.row0 * TT + t]);
-                continue;
-            }
-            float y = cur[op.row1 * TT + t];
-            int ta = t - op.lag, tb = ta - 1;
-            float xa = (ta >= 0) ? cur[op.row0 * TT + ta] : hist[op.hist_off + ((s_tile + ta) & op.hist_mask)];
-            float xb = (tb >= 0) ? cur[op.row0 * TT + tb] : hist[op.hist_off + ((s_tile + tb) & op.hist_mask)];
-            float o0 = bfly(xa, y);
-            float o1 = bfly(xb, y);
-            if (op.kind == 0) {
-                nxt[op.row0 * TT + t] = o0;
-                nxt[op.row1 * TT + t] = o1;
-            }
-            if (op.out0 >= 0) out(op.out0, t, o0);
-            if (op.out1 >= 0) out(op.out1, t, o1);
-        }
-        __syncthreads();
-
-        // Save the newest samples of each butterfly's row0 input for the following tiles.
-        for (int it = tid; it < nitems; it += nthr) {
-            const TreeOp op = ops[ob + it / TT];
-            int t = it % TT;
-            if (op.kind == 2) continue;
-            if (t >= TT - (op.hist_mask + 1))
-                hist[op.hist_off + ((s_tile + t) & op.hist_mask)] = cur[op.row0 * TT + t];
-        }
-        __syncthreads();
-
-        if (ph < nsteps) {
-            float *tmp = cur; cur = nxt; nxt = tmp;
-        }
-    }
-    return cur;
+    return __shfl_sync(kFull, (lane < 32 - L) ? x : p, (lane - L) & 31);
 }
 
-
-struct NoOut { __device__ void operator()(int, int, float) const { } };
-
-
-template<typename Ts>
-__global__ void __launch_bounds__(kTreeThreads) stage1_kernel(Stage1Args a)
+template<int K> struct RT
 {
-    constexpr int TT = kTreeTile;
-    extern __shared__ float sm[];
-    const int nrows = a.nrows, tid = threadIdx.x, nthr = blockDim.x;
-    float *bufA = sm, *bufB = sm + nrows * TT;
-    int *rowpos = (int *) (bufB + nrows * TT);
+    static constexpr int N = 1 << K;
+    static constexpr int NP = (K > 0) ? (1 << (K - 1)) : 1;
+    static constexpr int NS = (K > 0) ? K : 1;
+};
 
+// All K steps of a register tree, in place. pv[r][q] holds pair q's row0 input of the previous tile.
+template<int K>
+__device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>::NS][RT<K>::NP], int lane)
+{
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+#pragma unroll
+        for (int q = 0; q < RT<K>::NP; q++) {
+            const int h = 1 << r;
+            const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
+            const int L = rt_lag(r, q);
+            float x = v[i0], y = v[i0 + h];
+            float a = (L == 0) ? x : lagged(x, pv[r][q], L, lane);
+            float b = lagged(x, pv[r][q], L + 1, lane);
+            v[i0] = bfly(a, y);
+            v[i0 + h] = bfly(b, y);
+            pv[r][q] = x;
+        }
+    }
+}
+
+// Persistent histories: pair (r, q) needs its previous-tile row0 only in lanes >= 31 - lag.
+template<int K>
+__device__ __forceinline__ void rt_load(float (&pv)[RT<K>::NS][RT<K>::NP], const float *st, int lane)
+{
+    int off = 0;
+#pragma unroll
+    for (int r = 0; r < K; r++)
+#pragma unroll
+        for (int q = 0; q < RT<K>::NP; q++) {
+            const int L = rt_lag(r, q);
+            int i = lane - (31 - L);
+            pv[r][q] = (i >= 0) ? st[off + i] : 0.0f;
+            off += L + 1;
+        }
+}
+
+template<int K>
+__device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP], float *st, int lane)
+{
+    int off = 0;
+#pragma unroll
+    for (int r = 0; r < K; r++)
+#pragma unroll
+        for (int q = 0; q < RT<K>::NP; q++) {
+            const int L = rt_lag(r, q);
+            int i = lane - (31 - L);
+            if (i >= 0) st[off + i] = pv[r][q];
+            off += L + 1;
+        }
+}
+
+// Delay line between the phases, in shared memory: row rr = f * 2^RA + d (f < 2^RB) has capacity
+// P(f, d) + 32; 'pos' is the row's write position for the current tile.
+struct RingTab
+{
+    int *off, *cap, *pos;
+};
+
+template<int RA, int RB>
+__device__ __forceinline__ int ring_lag(int f, int d) { return ((1 << RB) - 1 - f) * brev_bits(d, RA); }
+
+template<int RA, int RB>
+__device__ void ring_init(RingTab &t, int *sm_int, long s0)
+{
+    constexpr int NR = 1 << (RA + RB);
+    t.off = sm_int;
+    t.cap = sm_int + NR;
+    t.pos = sm_int + 2 * NR;
+    if (threadIdx.x == 0) {
+        int o = 0;
+        for (int rr = 0; rr < NR; rr++) {
+            int c = ring_lag<RA, RB>(rr >> RA, rr & ((1 << RA) - 1)) + 32;
+            t.off[rr] = o;
+            t.cap[rr] = c;
+            t.pos[rr] = int(s0 % c);
+            o += c;
+        }
+    }
+}
+
+__device__ __forceinline__ int wrap_add(int p, int cap) { return (p >= cap) ? (p - cap) : ((p < 0) ? (p + cap) : p); }
+
+template<typename Ts, int RA, int RB>
+__global__ void __launch_bounds__(tree_threads(RA + RB)) stage1_kernel(Stage1Args a)
+{
+    constexpr int NA = 1 << RA, NB = 1 << RB, NR = 1 << (RA + RB);
+    constexpr int RING = ring_floats(RA, RB);
+    extern __shared__ long long sm_ll[];
+    int *sm_int = (int *) sm_ll;
+    RingTab tab;
+    int *opos = sm_int + 3 * NR;                    // output delay-line write positions, by final row
+    float *ring = (float *) (sm_int + 4 * NR);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
-    float *hist = a.hist + ((long) bt * gridDim.x + blk) * a.hist_per_block;
+    float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
     const Ts *in = (const Ts *) a.in + (long) (a.in_beam0 + b) * a.in_beam_stride;
-    Ts *ring = (Ts *) a.ring + (long) bt * a.ring_beam_stride;
+    Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride;
+    const long *out_off = a.ring_off + (long) blk * NR;
+    const int *out_cap = a.ring_cap + (long) blk * NR;
 
-    for (int n = tid; n < nrows; n += nthr)
-        rowpos[n] = int(a.s0 % (long) a.ring_cap[blk * nrows + n]);
+    ring_init<RA, RB>(tab, sm_int, a.s0);
+    for (int i = threadIdx.x; i < NR; i += blockDim.x)
+        opos[i] = int(a.s0 % out_cap[i]);
+    for (int i = threadIdx.x; i < RING; i += blockDim.x)
+        ring[i] = st[i];
+
+    const bool in_a = warp < NB, in_b = warp < NA;
+    float pva[RT<RA>::NS][RT<RA>::NP], pvb[RT<RB>::NS][RT<RB>::NP];
+    const float *sta = st + RING + warp * rt_state(RA);
+    const float *stb = st + RING + NB * rt_state(RA) + warp * rt_state(RB);
+    if (in_a) rt_load<RA>(pva, sta, lane);
+    if (in_b) rt_load<RB>(pvb, stb, lane);
     __syncthreads();
 
-    const int ntiles = a.nt / TT;
+    // Phase-a input rows c = blk*NR + warp*NA + i, lag(c) = in_lag0 - in_lag1*(warp*NA + i).
+    const long rowbase = ((long) blk * NR + warp * NA) * a.in_row_stride;
+    float nxt[NA];
+    if (in_a) {
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+            int lag = a.in_lag0 - a.in_lag1 * (warp * NA + i);
+            nxt[i] = to_f(in[rowbase + i * a.in_row_stride + ((a.in_s0 + lane - lag) & a.in_mask)]);
+        }
+    }
+
+    const int ntiles = a.nt / 32;
     for (int tile = 0; tile < ntiles; tile++) {
-        long s_tile = a.s0 + (long) tile * TT;
-        long s_in = a.in_s0 + (long) tile * TT;
-
-        for (int it = tid; it < nrows * TT; it += nthr) {
-            int n = it / TT, t = it % TT;
-            long c = (long) blk * nrows + n;
-            int lag = a.in_lag0 - a.in_lag1 * n;
-            bufA[it] = to_f(in[c * a.in_row_stride + ((s_in + t - lag) & a.in_mask)]);
+        if (in_a) {
+            float v[NA];
+#pragma unroll
+            for (int i = 0; i < NA; i++) v[i] = nxt[i];
+            if (tile + 1 < ntiles) {
+                long s_in = a.in_s0 + (long) (tile + 1) * 32 + lane;
+#pragma unroll
+                for (int i = 0; i < NA; i++) {
+                    int lag = a.in_lag0 - a.in_lag1 * (warp * NA + i);
+                    nxt[i] = to_f(in[rowbase + i * a.in_row_stride + ((s_in - lag) & a.in_mask)]);
+                }
+            }
+            rt_steps<RA>(v, pva, lane);
+#pragma unroll
+            for (int i = 0; i < NA; i++) {
+                int rr = warp * NA + i;
+                ring[tab.off[rr] + wrap_add(tab.pos[rr] + lane, tab.cap[rr])] = v[i];
+            }
         }
         __syncthreads();
-
-        float *res = run_program(bufA, bufB, a.ops, a.phase_begin, a.nphases, a.nphases, hist, s_tile, NoOut());
-
-        for (int it = tid; it < nrows * TT; it += nthr) {
-            int n = it / TT, t = it % TT;
-            int row = blk * nrows + n;
-            int cap = a.ring_cap[row];
-            int p = rowpos[n] + t;
-            if (p >= cap) p -= cap;
-            ring[a.ring_off[row] + p] = from_f<Ts>(res[it]);
-        }
-        __syncthreads();
-
-        for (int n = tid; n < nrows; n += nthr) {
-            int cap = a.ring_cap[blk * nrows + n];
-            int p = rowpos[n] + TT;
-            rowpos[n] = (p >= cap) ? (p - cap) : p;
+        if (in_b) {
+            float v[NB];
+#pragma unroll
+            for (int f = 0; f < NB; f++) {
+                int rr = f * NA + warp;
+                int p = tab.pos[rr] + lane - ring_lag<RA, RB>(f, warp);
+                v[f] = ring[tab.off[rr] + wrap_add(p, tab.cap[rr])];
+            }
+            __syncwarp();
+            if (lane < NB) {
+                int rr = lane * NA + warp;
+                tab.pos[rr] = wrap_add(tab.pos[rr] + 32, tab.cap[rr]);
+            }
+            rt_steps<RB>(v, pvb, lane);
+#pragma unroll
+            for (int f = 0; f < NB; f++) {
+                int i = (f << RA) | warp;
+                out[out_off[i] + wrap_add(opos[i] + lane, out_cap[i])] = from_f<Ts>(v[f]);
+            }
+            __syncwarp();
+            if (lane < NB) {
+                int i = (lane << RA) | warp;
+                opos[i] = wrap_add(opos[i] + 32, out_cap[i]);
+            }
         }
         __syncthreads();
     }
+
+    for (int i = threadIdx.x; i < RING; i += blockDim.x)
+        st[i] = ring[i];
+    if (in_a) rt_save<RA>(pva, (float *) sta, lane);
+    if (in_b) rt_save<RB>(pvb, (float *) stb, lane);
 }
 
 
+// Phase b of a stage-2 (subband) tree: before step r' (r' = 0..RB-1) and after it, subband rows of
+// pf level r'+1 are emitted (FrequencySubbands multiplet order), reproducing ReferenceTree::dedisperse_2d
+// (src_lib/ReferenceTree.cpp:120-300): even band pairs coincide with the in-place butterflies, odd
+// ("staggered") pairs (2k+1, 2k+2) are extra butterflies with their own histories ps[r'][u].
+template<int RB, bool STAG, typename Emit>
+__device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv)[RT<RB>::NS][RT<RB>::NP],
+                                                 float (&ps)[RT<RB>::NS][RT<RB>::NP], const Stage2Args &a,
+                                                 int lane, Emit emit)
+{
+    constexpr int NB = 1 << RB;
+#pragma unroll
+    for (int f = 0; f < NB; f++)
+        if (f < a.sb_count[0]) emit(a.sb_mbase[0] + f, v[f]);
+
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        const int cnt = a.sb_count[r + 1], mb = a.sb_mbase[r + 1];
+        const int h = 1 << r;
+#pragma unroll
+        for (int u = 0; u < (STAG ? st_count(RB, r) : 0); u++) {
+            const int k = u >> r, j = u & (h - 1);
+            if (2 * k + 1 < cnt) {
+                const int qa = ((2 * k + 1) << r) | j, qb = ((2 * k + 2) << r) | j;
+                const int L = rt_lag(r, j);
+                float x = v[qa], y = v[qb];
+                float aa = (L == 0) ? x : lagged(x, ps[r][u], L, lane);
+                float bb = lagged(x, ps[r][u], L + 1, lane);
+                int m = mb + (2 * k + 1) * (2 << r) + 2 * bitrev_c(j, r);
+                emit(m, bfly(aa, y));
+                emit(m + 1, bfly(bb, y));
+                ps[r][u] = x;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RT<RB>::NP; q++) {
+            const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
+            const int k = q >> r, j = q & (h - 1);
+            const int L = rt_lag(r, q);
+            float x = v[i0], y = v[i0 + h];
+            float aa = (L == 0) ? x : lagged(x, pv[r][q], L, lane);
+            float bb = lagged(x, pv[r][q], L + 1, lane);
+            float o0 = bfly(aa, y), o1 = bfly(bb, y);
+            v[i0] = o0;
+            v[i0 + h] = o1;
+            pv[r][q] = x;
+            if (2 * k < cnt) {
+                int m = mb + (2 * k) * (2 << r) + 2 * bitrev_c(j, r);
+                emit(m, o0);
+                emit(m + 1, o1);
+            }
+        }
+    }
+}
+
+template<int K>
+__device__ __forceinline__ void st_load(float (&ps)[RT<K>::NS][RT<K>::NP], const float *st, int lane)
+{
+    int off = 0;
+#pragma unroll
+    for (int r = 0; r < K; r++)
+#pragma unroll
+        for (int u = 0; u < RT<K>::NP; u++) {
+            if (u < st_count(K, r)) {
+                const int L = rt_lag(r, u & ((1 << r) - 1));
+                int i = lane - (31 - L);
+                ps[r][u] = (i >= 0) ? st[off + i] : 0.0f;
+                off += L + 1;
+            } else {
+                ps[r][u] = 0.0f;
+            }
+        }
+}
+
+template<int K>
+__device__ __forceinline__ void st_save(const float (&ps)[RT<K>::NS][RT<K>::NP], float *st, int lane)
+{
+    int off = 0;
+#pragma unroll
+    for (int r = 0; r < K; r++)
+#pragma unroll
+        for (int u = 0; u < RT<K>::NP; u++) {
+            if (u < st_count(K, r)) {
+                const int L = rt_lag(r, u & ((1 << r) - 1));
+                int i = lane - (31 - L);
+                if (i >= 0) st[off + i] = ps[r][u];
+                off += L + 1;
+            }
+        }
+}
+
 template<typename Ts>
-struct PfRingOut
+struct PfEmit
 {
     Ts *pf;
-    long rowbase, cap_mask, s_tile, cap;
-    __device__ void operator()(int o, int t, float v) const
+    long rowbase, cap, mask, s;
+    __device__ __forceinline__ void operator()(int m, float v) const
     {
-        pf[(rowbase + o) * cap + ((s_tile + t) & cap_mask)] = from_f<Ts>(v);
+        pf[(rowbase + m) * cap + (s & mask)] = from_f<Ts>(v);
     }
 };
 
-
-template<typename Ts>
-__global__ void __launch_bounds__(kTreeThreads) stage2_kernel(Stage2Args a)
+template<typename Ts, int RA, int RB, bool STAG>
+__global__ void __launch_bounds__(tree_threads(RA + RB)) stage2_kernel(Stage2Args a)
 {
-    constexpr int TT = kTreeTile;
-    extern __shared__ float sm[];
-    const int nrows = a.nrows, tid = threadIdx.x, nthr = blockDim.x;
-    float *bufA = sm, *bufB = sm + nrows * TT;
-    int *rowpos = (int *) (bufB + nrows * TT);
+    constexpr int NA = 1 << RA, NB = 1 << RB, NR = 1 << (RA + RB);
+    constexpr int RING = ring_floats(RA, RB);
+    extern __shared__ long long sm_ll[];
+    long *ioff = (long *) sm_ll;                    // offset of the input delay line of row a
+    int *sm_int = (int *) (ioff + NR);
+    RingTab tab;
+    int *ipos = sm_int + 3 * NR;                    // its next read position
+    int *icap = ipos + NR;                          // its capacity
+    float *ring = (float *) (icap + NR);
 
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int d = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
-    float *hist = a.hist + ((long) bt * gridDim.x + d) * a.hist_per_block;
-    const Ts *ring = (const Ts *) a.ring + (long) bt * a.ring_beam_stride;
+    float *st = a.state + ((long) bt * gridDim.x + d) * a.state_per_block;
+    const Ts *in = (const Ts *) a.ring + (long) bt * a.ring_beam_stride;
 
-    const long dm = brev_bits(d, a.amb_rank) + (a.uflag ? (1L << a.amb_rank) : 0L);
-    for (int r = tid; r < nrows; r += nthr) {
-        long lag = (long) (nrows - 1 - r) * dm;
-        long cap = a.ring_cap[(long) r * (1L << a.amb_rank) + d];
+    ring_init<RA, RB>(tab, sm_int, a.s0);
+    const long dm1 = brev_bits(d, a.amb_rank) + (a.uflag ? (1L << a.amb_rank) : 0L);
+    for (int r = threadIdx.x; r < NR; r += blockDim.x) {
+        long row = ((long) r << a.amb_rank) + d;
+        long lag = (long) (NR - 1 - r) * dm1;
+        long cap = a.ring_cap[row];
         long p = (a.s0 - lag) % cap;
-        rowpos[r] = int(p < 0 ? p + cap : p);
+        ipos[r] = int(p < 0 ? p + cap : p);
+        icap[r] = int(cap);
+        ioff[r] = a.ring_off[row];
+    }
+    for (int i = threadIdx.x; i < RING; i += blockDim.x)
+        ring[i] = st[i];
+
+    const bool in_a = warp < NB, in_b = warp < NA;
+    float pva[RT<RA>::NS][RT<RA>::NP], pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
+    const float *sta = st + RING + warp * rt_state(RA);
+    const float *stb = st + RING + NB * rt_state(RA) + warp * (rt_state(RB) + st_state(RB));
+    if (in_a) rt_load<RA>(pva, sta, lane);
+    if (in_b) {
+        rt_load<RB>(pvb, stb, lane);
+        if (STAG) st_load<RB>(psb, stb + rt_state(RB), lane);
     }
     __syncthreads();
 
-    PfRingOut<Ts> out;
-    out.pf = (Ts *) a.pf;
-    out.rowbase = ((long) bt * a.ndm_out + ((long) brev_bits(d, a.amb_rank) << a.pf_shift)) * a.M;
-    out.cap = a.pf_cap;
-    out.cap_mask = a.pf_cap - 1;
+    float nxt[NA];
+    if (in_a) {
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+            int r = warp * NA + i;
+            nxt[i] = to_f(in[ioff[r] + wrap_add(ipos[r] + lane, icap[r])]);
+        }
+    }
 
-    const int ntiles = a.nt / TT;
+    PfEmit<Ts> emit;
+    emit.pf = (Ts *) a.pf;
+    emit.cap = a.pf_cap;
+    emit.mask = a.pf_cap - 1;
+    const int pf_dm = brev_bits(warp, RA);
+    emit.rowbase = ((long) bt * a.ndm_out + ((long) brev_bits(d, a.amb_rank) << RA) + pf_dm) * a.M;
+
+    const int ntiles = a.nt / 32;
     for (int tile = 0; tile < ntiles; tile++) {
-        long s_tile = a.s0 + (long) tile * TT;
-        out.s_tile = s_tile;
-
-        for (int it = tid; it < nrows * TT; it += nthr) {
-            int r = it / TT, t = it % TT;
-            long row = (long) r * (1L << a.amb_rank) + d;
-            int cap = a.ring_cap[row];
-            int p = rowpos[r] + t;
-            if (p >= cap) p -= cap;
-            bufA[it] = to_f(ring[a.ring_off[row] + p]);
+        if (in_a) {
+            float v[NA];
+#pragma unroll
+            for (int i = 0; i < NA; i++) v[i] = nxt[i];
+            if (tile + 1 < ntiles) {
+#pragma unroll
+                for (int i = 0; i < NA; i++) {
+                    int r = warp * NA + i;
+                    int c = icap[r];
+                    int p = wrap_add(ipos[r] + 32, c);
+                    nxt[i] = to_f(in[ioff[r] + wrap_add(p + lane, c)]);
+                    __syncwarp();
+                    if (lane == 0) ipos[r] = p;
+                }
+            }
+            rt_steps<RA>(v, pva, lane);
+#pragma unroll
+            for (int i = 0; i < NA; i++) {
+                int rr = warp * NA + i;
+                ring[tab.off[rr] + wrap_add(tab.pos[rr] + lane, tab.cap[rr])] = v[i];
+            }
         }
         __syncthreads();
-
-        run_program(bufA, bufB, a.ops, a.phase_begin, a.nphases, a.dd_rank, hist, s_tile, out);
-
-        for (int r = tid; r < nrows; r += nthr) {
-            int cap = a.ring_cap[(long) r * (1L << a.amb_rank) + d];
-            int p = rowpos[r] + TT;
-            rowpos[r] = (p >= cap) ? (p - cap) : p;
+        if (in_b) {
+            float v[NB];
+#pragma unroll
+            for (int f = 0; f < NB; f++) {
+                int rr = f * NA + warp;
+                int p = tab.pos[rr] + lane - ring_lag<RA, RB>(f, warp);
+                v[f] = ring[tab.off[rr] + wrap_add(p, tab.cap[rr])];
+            }
+            __syncwarp();
+            if (lane < NB) {
+                int rr = lane * NA + warp;
+                tab.pos[rr] = wrap_add(tab.pos[rr] + 32, tab.cap[rr]);
+            }
+            emit.s = a.s0 + (long) tile * 32 + lane;
+            phase_b_subbands<RB, STAG>(v, pvb, psb, a, lane, emit);
         }
         __syncthreads();
+    }
+
+    for (int i = threadIdx.x; i < RING; i += blockDim.x)
+        st[i] = ring[i];
+    if (in_a) rt_save<RA>(pva, (float *) sta, lane);
+    if (in_b) {
+        rt_save<RB>(pvb, (float *) stb, lane);
+        if (STAG) st_save<RB>(psb, (float *) stb + rt_state(RB), lane);
     }
 }
 
@@ -422,7 +660,6 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_fl
 
     const int tout = tout0 + lane;
     const bool active = (lane < ntw);
-    const int pf_dm = dm & ((1 << a.pf_shift) - 1);
     const int Wds = a.ndm_out / a.ndm_wt, Tds = a.nt_out / a.nt_wt;
     const float *wp = a.wt + ((((long) b * a.ndm_wt + dm / Wds) * a.nt_wt + (active ? tout / Tds : 0)) * a.P) * a.N;
     const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
@@ -435,7 +672,7 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_fl
 
     for (int m = 0; m < a.M; m++) {
         const Ts *row = pfrows + (long) m * a.pf_cap;
-        long s_base = a.s0 + R0 - a.final_lag[pf_dm * a.M + m];
+        long s_base = a.s0 + R0;
         for (int u = lane; u < len0; u += 32)
             lev[u] = to_f(row[(s_base + u) & mask]);
         __syncwarp();
@@ -540,7 +777,8 @@ void launch_lds(const LdsArgs &a, int dtype, cudaStream_t s)
     else launch_lds_d<__nv_bfloat16>(a, s);
 }
 
-static size_t tree_smem(int nrows) { return (size_t) 2 * nrows * kTreeTile * sizeof(float) + nrows * sizeof(int); }
+template<int RA, int RB>
+static size_t tree_smem() { return (size_t) ring_floats(RA, RB) * sizeof(float) + 8 * (1 << (RA + RB)) * sizeof(int); }
 
 template<typename K>
 static void set_smem(K kernel, size_t bytes)
@@ -549,13 +787,30 @@ static void set_smem(K kernel, size_t bytes)
     if (e != cudaSuccess) throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
 }
 
+template<typename Ts, int R>
+static void launch_stage1_r(const Stage1Args &a, int nblocks, int B, cudaStream_t s)
+{
+    constexpr int RA = split_ra(R), RB = split_rb(R);
+    size_t sm = tree_smem<RA, RB>();
+    set_smem(stage1_kernel<Ts, RA, RB>, sm);
+    stage1_kernel<Ts, RA, RB><<<dim3(nblocks, B), tree_threads(R), sm, s>>>(a);
+    check_launch("stage1_kernel");
+}
+
 template<typename Ts>
 static void launch_stage1_t(const Stage1Args &a, int nblocks, int B, cudaStream_t s)
 {
-    size_t sm = tree_smem(a.nrows);
-    set_smem(stage1_kernel<Ts>, sm);
-    stage1_kernel<Ts><<<dim3(nblocks, B), kTreeThreads, sm, s>>>(a);
-    check_launch("stage1_kernel");
+    switch (a.rank) {
+    case 1: launch_stage1_r<Ts, 1>(a, nblocks, B, s); break;
+    case 2: launch_stage1_r<Ts, 2>(a, nblocks, B, s); break;
+    case 3: launch_stage1_r<Ts, 3>(a, nblocks, B, s); break;
+    case 4: launch_stage1_r<Ts, 4>(a, nblocks, B, s); break;
+    case 5: launch_stage1_r<Ts, 5>(a, nblocks, B, s); break;
+    case 6: launch_stage1_r<Ts, 6>(a, nblocks, B, s); break;
+    case 7: launch_stage1_r<Ts, 7>(a, nblocks, B, s); break;
+    case 8: launch_stage1_r<Ts, 8>(a, nblocks, B, s); break;
+    default: throw std::runtime_error("stage1_kernel: unsupported dd rank " + std::to_string(a.rank));
+    }
 }
 
 void launch_stage1(const Stage1Args &a, int dtype, int nblocks, int B, cudaStream_t s)
@@ -565,13 +820,37 @@ void launch_stage1(const Stage1Args &a, int dtype, int nblocks, int B, cudaStrea
     else launch_stage1_t<__nv_bfloat16>(a, nblocks, B, s);
 }
 
+template<typename Ts, int R>
+static void launch_stage2_r(const Stage2Args &a, int nblocks, int B, cudaStream_t s)
+{
+    constexpr int RA = split_ra(R), RB = split_rb(R);
+    size_t sm = tree_smem<RA, RB>();
+    bool stag = false;
+    for (int l = 1; l <= RB; l++) stag = stag || (a.sb_count[l] >= 2);
+    if (stag) {
+        set_smem(stage2_kernel<Ts, RA, RB, true>, sm);
+        stage2_kernel<Ts, RA, RB, true><<<dim3(nblocks, B), tree_threads(R), sm, s>>>(a);
+    } else {
+        set_smem(stage2_kernel<Ts, RA, RB, false>, sm);
+        stage2_kernel<Ts, RA, RB, false><<<dim3(nblocks, B), tree_threads(R), sm, s>>>(a);
+    }
+    check_launch("stage2_kernel");
+}
+
 template<typename Ts>
 static void launch_stage2_t(const Stage2Args &a, int nblocks, int B, cudaStream_t s)
 {
-    size_t sm = tree_smem(a.nrows);
-    set_smem(stage2_kernel<Ts>, sm);
-    stage2_kernel<Ts><<<dim3(nblocks, B), kTreeThreads, sm, s>>>(a);
-    check_launch("stage2_kernel");
+    switch (a.rank) {
+    case 1: launch_stage2_r<Ts, 1>(a, nblocks, B, s); break;
+    case 2: launch_stage2_r<Ts, 2>(a, nblocks, B, s); break;
+    case 3: launch_stage2_r<Ts, 3>(a, nblocks, B, s); break;
+    case 4: launch_stage2_r<Ts, 4>(a, nblocks, B, s); break;
+    case 5: launch_stage2_r<Ts, 5>(a, nblocks, B, s); break;
+    case 6: launch_stage2_r<Ts, 6>(a, nblocks, B, s); break;
+    case 7: launch_stage2_r<Ts, 7>(a, nblocks, B, s); break;
+    case 8: launch_stage2_r<Ts, 8>(a, nblocks, B, s); break;
+    default: throw std::runtime_error("stage2_kernel: unsupported dd rank " + std::to_string(a.rank));
+    }
 }
 
 void launch_stage2(const Stage2Args &a, int dtype, int nblocks, int B, cudaStream_t s)

@@ -5,54 +5,37 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "regtree.cuh"
+
 namespace pb2 {
 
-// Tree samples per tile in the tree kernels (one warp-wide run of samples per row).
-constexpr int kTreeTile = 32;
-constexpr int kTreeThreads = 512;
-constexpr int kMaxTreeRows = 256;   // 2^8: stage ranks are <= 8 for tree rank <= 16
+// Split of a rank-R tree into register trees: phase b takes the upper RB = ceil(R/2) row bits (for a
+// stage-2 tree this is its peak-finding rank, so subband rows come out of phase b aligned).
+__host__ __device__ constexpr int split_rb(int R) { return (R + 1) / 2; }
+__host__ __device__ constexpr int split_ra(int R) { return R - (R + 1) / 2; }
 
-// One operation of a tree "program". A program is a list of phases; phase k is
-// ops[phase_begin[k] .. phase_begin[k+1]) and all ops of a phase read the rows as they were at the
-// start of the phase.
-//
-//  kind 0 (butterfly, in place):  row0' = (row0[t-lag]   + row1[t]) / sqrt2
-//                                 row1' = (row0[t-lag-1] + row1[t]) / sqrt2
-//  kind 1 (staggered butterfly):  same arithmetic, results only go to outputs out0/out1
-//  kind 2 (copy):                 out0 = row0[t]
-//
-// Butterflies keep the last (lag+1) samples of their row0 input in a history delay line of
-// capacity hist_mask+1 (a power of two) at offset hist_off of the block's history area.
-// out0/out1 >= 0 name subband output rows (stage-2 programs), -1 for none.
-struct TreeOp
+// Threads per block of a two-phase tree kernel of rank R (one warp per register-tree group).
+__host__ __device__ constexpr int tree_threads(int R)
 {
-    int16_t row0, row1;
-    int16_t kind, pad;
-    int32_t lag;
-    int32_t hist_off;
-    int32_t hist_mask;
-    int32_t out0, out1;
-};
+    return 32 * ((split_ra(R) > split_rb(R)) ? (1 << split_ra(R)) : (1 << split_rb(R)));
+}
 
-// Arguments of the stage-1 tree kernel (one primary tree).
+// Stage 1 (one primary tree): input rows -> two-phase tree -> per-row output delay lines.
 struct Stage1Args
 {
-    const TreeOp *ops;
-    const int *phase_begin;
-    int nphases;
-    int nrows;              // 2^stage1_dd_rank
-    long hist_per_block;    // floats of history per (beam, block)
-    float *hist;            // (total_beams, nblocks, hist_per_block)
+    int rank;               // stage-1 dd rank (rows per block = 2^rank)
+    long state_per_block;   // floats
+    float *state;           // (total_beams, nblocks, state_per_block)
 
-    // Input rows: element (b, row c, time s) at in + b*in_beam_stride + c*in_row_stride + ((s - lag(c)) & in_mask),
-    // lag(c) = in_lag0 - in_lag1 * (c % nrows); s counts samples of this tree's time base.
+    // Input element (b, row c, time s) at in + (in_beam0 + b)*in_beam_stride + c*in_row_stride + ((s - lag(c)) & in_mask),
+    // lag(c) = in_lag0 - in_lag1 * (c mod 2^rank).
     const void *in;
     long in_beam_stride, in_row_stride, in_mask;
     long in_s0;             // time of the chunk's first sample in the input's indexing
     int in_lag0, in_lag1;
-    int in_beam0;           // beam index of batch beam 0 in the input (0 for per-batch buffers)
+    int in_beam0;
 
-    // Output delay lines: row (a, n) -> ring + b*ring_beam_stride + ring_off[row], capacity ring_cap[row].
+    // Output delay lines: row (a, n) -> ring + bt*ring_beam_stride + ring_off[row], capacity ring_cap[row].
     void *ring;
     const long *ring_off;
     const int *ring_cap;
@@ -63,15 +46,12 @@ struct Stage1Args
     int beam0;              // total-beam index of batch beam 0
 };
 
-// Arguments of the stage-2 tree kernel (one output tree).
+// Stage 2 (one output tree): stage-1 delay lines -> two-phase subband tree -> peak-finder delay lines.
 struct Stage2Args
 {
-    const TreeOp *ops;
-    const int *phase_begin;
-    int nphases;
-    int nrows;              // 2^tree.dd_rank
-    long hist_per_block;
-    float *hist;            // (total_beams, 2^amb_rank, hist_per_block)
+    int rank;               // stage-2 dd rank (rows per block = 2^rank)
+    long state_per_block;
+    float *state;           // (total_beams, 2^amb_rank, state_per_block)
 
     // Input: stage-1 delay lines of the primary tree; row (a, d) = a * 2^amb_rank + d.
     const void *ring;
@@ -79,14 +59,16 @@ struct Stage2Args
     const int *ring_cap;
     long ring_beam_stride;
     int amb_rank;           // stage-2 ambient rank (= stage-1 dd rank)
-    int dd_rank;            // stage-2 active rank (= rows)
     int uflag;              // 1 for downsampled primary trees (upper half of the DM range)
 
-    // Output: peak-finder delay lines, row ((b*ndm_out + dm) * M + m), capacity pf_cap (power of two).
+    // Subbands: counts per pf level (0..pf_rank) and first multiplet index of each level.
+    int sb_count[5];
+    int sb_mbase[5];
+
+    // Output: peak-finder delay lines, row ((bt*ndm_out + dm) * M + m), capacity pf_cap (power of two).
     void *pf;
     int M;
     int ndm_out;
-    int pf_shift;           // dd_rank - pf_rank: coarse dm of block d starts at bitrev(d) << pf_shift
     long pf_cap;
 
     long s0;
@@ -97,17 +79,15 @@ struct Stage2Args
 // Arguments of the peak-finding kernel (one output tree).
 struct PfArgs
 {
-    const void *pf;         // delay lines written by the stage-2 kernel
+    const void *pf;         // delay lines written by the stage-2 kernel (subband-aligned)
     long pf_cap;
     const float *wt;        // (B, ndm_wt, nt_wt, P, N) for this batch
     void *out_max;          // (B, ndm_out, nt_out), storage dtype
     uint32_t *out_argmax;   // (B, ndm_out, nt_out)
     const int *m_to_n;      // (M,)
-    const int *final_lag;   // (2^pf_shift, M): subband alignment lag of (pf_dm, m)
     int M, N, P, L;         // multiplets, subbands, profiles, boxcar levels
     int ndm_out, nt_out, ndm_wt, nt_wt;
     int Dout, Dcore, tpad;
-    int pf_shift;
     long s0;                // stream time of the chunk's first sample
     int beam0;
 };
@@ -135,6 +115,10 @@ struct LdsArgs
     long ichunk;
     int beam0, B, total_beams;
 };
+
+// Floats of persistent state per block of the stage kernels (host and device agree by construction).
+inline long stage1_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), false); }
+inline long stage2_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), true); }
 
 void launch_grid(const GridArgs &a, int dtype, int B, cudaStream_t s);
 void launch_lds(const LdsArgs &a, int dtype, cudaStream_t s);
