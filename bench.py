@@ -33,11 +33,11 @@ METRIC = "real-time beams/B200 (rank 16, fp16)"
 L2_BYTES = 126 * 2 ** 20
 
 
-def bench_config(beams, dtype):
+def bench_config(beams, dtype, rank=16, npri=5, nfreq=16384):
     prim = [dict(num_early_triggers=0, max_width=32, dm_downsampling=0, time_downsampling=0,
-                 wt_dm_downsampling=64, wt_time_downsampling=64) for _ in range(5)]
-    return dict(zone_nfreq=[16384], zone_freq_edges=[400.0, 800.0], time_sample_ms=SAMPLE_MS,
-                toplevel_tree_rank=16, time_samples_per_chunk=CHUNK, dtype=dtype,
+                 wt_dm_downsampling=64, wt_time_downsampling=64) for _ in range(npri)]
+    return dict(zone_nfreq=[nfreq], zone_freq_edges=[400.0, 800.0], time_sample_ms=SAMPLE_MS,
+                toplevel_tree_rank=rank, time_samples_per_chunk=CHUNK, dtype=dtype,
                 frequency_subband_counts=[0, 0, 0, 0, 1], primary_trees=prim,
                 beams_per_gpu=beams, beams_per_batch=beams, num_active_batches=1,
                 future_write_max_samples=0, max_gpu_clag=10000)
@@ -115,7 +115,7 @@ def run_ours(args, rank, world):
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    cfg = bench_config(args.beams, args.dtype)
+    cfg = bench_config(args.beams, args.dtype, args.rank, args.npri, args.nfreq)
     plan = pb.DedispersionPlan(pb.DedispersionConfig.from_dict(cfg))
     dd = pb.GpuDedisperser(plan, cuda_device_id=dev, num_consumers=1)
     dd.allocate()
@@ -285,6 +285,10 @@ def main():
     ap.add_argument("--dtype", default="float16", choices=["float16", "bfloat16", "float32"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # Smaller workloads, for profiler captures only (the headline workload is the default).
+    ap.add_argument("--rank", type=int, default=16)
+    ap.add_argument("--npri", type=int, default=5)
+    ap.add_argument("--nfreq", type=int, default=16384)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

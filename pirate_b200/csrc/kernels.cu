@@ -18,6 +18,7 @@
 #include <cuda_fp16.h>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 namespace pb2 {
 
@@ -603,43 +604,83 @@ __global__ void __launch_bounds__(tree_threads(RA + RB)) stage2_kernel(Stage2Arg
 constexpr int kPfWarps = 4;
 constexpr int kPfMaxLevels = 6;
 
-struct PfLevels
-{
-    int L;
-    int dt[kPfMaxLevels], n[kPfMaxLevels], off[kPfMaxLevels], r[kPfMaxLevels], s[kPfMaxLevels];
-    int total;
-};
-
-__device__ __forceinline__ void pf_levels(const PfArgs &a, int len0, PfLevels &lv)
-{
-    lv.L = a.L;
-    int off = 0;
-    for (int l = 0; l < a.L; l++) {
-        int dt = min(a.Dcore, 1 << l);
-        lv.dt[l] = dt;
-        lv.n[l] = (len0 - (1 << l)) / dt + 1;
-        lv.off[l] = off;
-        off += lv.n[l];
-    }
-    for (int l = 0; l + 1 < a.L; l++) {
-        lv.r[l] = lv.dt[l + 1] / lv.dt[l];
-        lv.s[l] = (1 << l) / lv.dt[l];
-    }
-    lv.total = off;
-}
-
-struct PfBest
-{
-    float v;
-    int key;
-    uint32_t tok;
-    __device__ __forceinline__ void update(float val, int k, uint32_t t)
-    {
-        if ((val > v) || (val == v && k < key)) { v = val; key = k; tok = t; }
-    }
-};
+// Number of entries of boxcar level l in a window of len0 samples (level 0 = samples).
+__device__ __forceinline__ int pf_nlev(int len0, int l, int dt) { return (len0 - (1 << l)) / dt + 1; }
 
 template<typename Ts>
+__device__ __forceinline__ float ld_f(const Ts *p) { return to_f(*p); }
+
+// Loads multiplet row 'row' over the warp's window into lev[0..len0) and builds boxcar levels
+// 1..L-1 after it with the reference recursion B_{l+1}[u] = B_l[r u] + B_l[r u + s].
+template<typename Ts, int L>
+__device__ __forceinline__ void pf_build(float *lev, int len0, int lane, int Dcore, const Ts *row, long s_base, long mask)
+{
+    for (int u = lane; u < len0; u += 32)
+        lev[u] = to_f(row[(s_base + u) & mask]);
+    __syncwarp();
+    int off = 0;
+#pragma unroll
+    for (int l = 0; l + 1 < L; l++) {
+        const int dt = min(Dcore, 1 << l), dt1 = min(Dcore, 1 << (l + 1));
+        const int n = pf_nlev(len0, l, dt), n1 = pf_nlev(len0, l + 1, dt1);
+        const int rr = dt1 / dt, ss = (1 << l) / dt;
+        const float *src = lev + off;
+        float *dst = lev + off + n;
+        for (int u = lane; u < n1; u += 32)
+            dst[u] = __fadd_rn(src[rr * u], src[rr * u + ss]);
+        __syncwarp();
+        off += n;
+    }
+}
+
+// Group (level l, multiplet m) of one output time: the reference scans fine times 'is' and, per fine
+// time, profiles p = 0 (level 0 only), 3l+1, 3l+2, 3l+3. Keeps the first maximum of the group.
+template<bool P0>
+__device__ __forceinline__ void pf_group(const float *x, int nsamp, int S, float w0, float w1, float w2, float w3,
+                                         bool full, float &gmax, int &gidx)
+{
+    gmax = -1.0e30f;
+    gidx = -1;
+    if (S == 1) {
+        float x0 = x[-3], x1 = x[-2], x2 = x[-1];
+        for (int is = 0; is < nsamp; is++) {
+            float x3 = x[is];
+            if (P0) { float v = __fmul_rn(w0, x3); if (v > gmax) { gmax = v; gidx = 4 * is; } }
+            if (full) {
+                float hx3 = __fmul_rn(0.5f, x3);
+                float v1 = __fmul_rn(w1, __fadd_rn(x2, x3));
+                float v2 = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3));
+                float v3 = __fmul_rn(w3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3));
+                if (v1 > gmax) { gmax = v1; gidx = 4 * is + 1; }
+                if (v2 > gmax) { gmax = v2; gidx = 4 * is + 2; }
+                if (v3 > gmax) { gmax = v3; gidx = 4 * is + 3; }
+            }
+            x0 = x1; x1 = x2; x2 = x3;
+        }
+    } else {
+        for (int is = 0; is < nsamp; is++) {
+            float x0 = x[is - 3 * S], x1 = x[is - 2 * S], x2 = x[is - S], x3 = x[is];
+            if (P0) { float v = __fmul_rn(w0, x3); if (v > gmax) { gmax = v; gidx = 4 * is; } }
+            if (full) {
+                float hx3 = __fmul_rn(0.5f, x3);
+                float v1 = __fmul_rn(w1, __fadd_rn(x2, x3));
+                float v2 = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3));
+                float v3 = __fmul_rn(w3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3));
+                if (v1 > gmax) { gmax = v1; gidx = 4 * is + 1; }
+                if (v2 > gmax) { gmax = v2; gidx = 4 * is + 2; }
+                if (v3 > gmax) { gmax = v3; gidx = 4 * is + 3; }
+            }
+        }
+    }
+}
+
+// One warp per (beam, coarse dm, 32 consecutive output times). For each multiplet the warp stages
+// the input window in shared memory and builds the boxcar levels (every boxcar sum has the
+// reference's rounding); each lane then scans the trials of its output time. Across groups the
+// winner is the first group, in the reference's scan order (level, multiplet), whose maximum equals
+// the overall maximum; within a group the first trial reaching it. This reproduces
+// ReferencePeakFindingKernel::apply's strict-'>' sequential scan (src_lib/PeakFindingKernel.cu:339-420).
+template<typename Ts, int L>
 __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_floats)
 {
     extern __shared__ float sm[];
@@ -651,12 +692,8 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_fl
         return;   // whole warp exits; warps never synchronize across the block
 
     const int ntw = min(32, a.nt_out - tout0);
-    const int R0 = tout0 * a.Dout - a.tpad;
     const int len0 = ntw * a.Dout + a.tpad;
     float *lev = sm + warp * warp_floats;
-
-    PfLevels lv;
-    pf_levels(a, len0, lv);
 
     const int tout = tout0 + lane;
     const bool active = (lane < ntw);
@@ -664,65 +701,53 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_fl
     const float *wp = a.wt + ((((long) b * a.ndm_wt + dm / Wds) * a.nt_wt + (active ? tout / Tds : 0)) * a.P) * a.N;
     const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
     const long mask = a.pf_cap - 1;
+    const long s_base = a.s0 + (long) tout0 * a.Dout - a.tpad;
+    const bool full = (a.P > 1);
 
-    PfBest best;
-    best.v = -1.0e30f;
-    best.key = -1;
-    best.tok = 0xffffffffu;
+    float best = -1.0e30f;
+    int win = 0x7fffffff;     // (l * M + m) * 256 + in-group index of the winning trial
 
     for (int m = 0; m < a.M; m++) {
-        const Ts *row = pfrows + (long) m * a.pf_cap;
-        long s_base = a.s0 + R0;
-        for (int u = lane; u < len0; u += 32)
-            lev[u] = to_f(row[(s_base + u) & mask]);
-        __syncwarp();
-        for (int l = 0; l + 1 < lv.L; l++) {
-            const float *src = lev + lv.off[l];
-            float *dst = lev + lv.off[l + 1];
-            int rr = lv.r[l], ss = lv.s[l];
-            for (int u = lane; u < lv.n[l + 1]; u += 32)
-                dst[u] = __fadd_rn(src[rr * u], src[rr * u + ss]);
-            __syncwarp();
-        }
-
+        pf_build<Ts, L>(lev, len0, lane, a.Dcore, pfrows + (long) m * a.pf_cap, s_base, mask);
         if (active) {
-            int n = a.m_to_n[m];
-            for (int l = 0; l < lv.L; l++) {
-                const int dt = lv.dt[l], S = (1 << l) / dt, nsamp = a.Dout / dt;
+            const int n = a.m_to_n[m];
+            int off = 0;
+#pragma unroll
+            for (int l = 0; l < L; l++) {
+                const int dt = min(a.Dcore, 1 << l), S = (1 << l) / dt, nsamp = a.Dout / dt;
                 const int I = (a.tpad + dt - (1 << l)) / dt;
-                const float *x = lev + lv.off[l] + I + lane * nsamp;
-                float w0 = (l == 0) ? wp[n] : 0.0f;
-                float w1 = 0.0f, w2 = 0.0f, w3 = 0.0f;
-                if (a.P > 1) {
+                const float *x = lev + off + I + lane * nsamp;
+                float w0 = (l == 0) ? wp[n] : 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f;
+                if (full) {
                     w1 = wp[(3 * l + 1) * a.N + n];
                     w2 = wp[(3 * l + 2) * a.N + n];
                     w3 = wp[(3 * l + 3) * a.N + n];
                 }
-                const int kbase = (l * a.M + m) * 64;
-                for (int is = 0; is < nsamp; is++) {
-                    float x0 = x[is - 3 * S], x1 = x[is - 2 * S], x2 = x[is - S], x3 = x[is];
-                    uint32_t tk0 = (uint32_t(m) << 16) | uint32_t(is * dt);
-                    int k = (kbase + is) * 4;
-                    if (l == 0)
-                        best.update(__fmul_rn(w0, x3), k, tk0);
-                    if (a.P > 1) {
-                        float y1 = __fadd_rn(x2, x3);
-                        float y2 = __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), __fmul_rn(0.5f, x3));
-                        float y3 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), __fmul_rn(0.5f, x3));
-                        best.update(__fmul_rn(w1, y1), k + 1, tk0 | (uint32_t(3 * l + 1) << 8));
-                        best.update(__fmul_rn(w2, y2), k + 2, tk0 | (uint32_t(3 * l + 2) << 8));
-                        best.update(__fmul_rn(w3, y3), k + 3, tk0 | (uint32_t(3 * l + 3) << 8));
-                    }
-                }
+                float gmax;
+                int gidx;
+                if (l == 0) pf_group<true>(x, nsamp, S, w0, w1, w2, w3, full, gmax, gidx);
+                else pf_group<false>(x, nsamp, S, w0, w1, w2, w3, full, gmax, gidx);
+                const int g = ((l * a.M + m) << 8) + gidx;
+                if (gidx >= 0 && (gmax > best || (gmax == best && g < win))) { best = gmax; win = g; }
+                off += pf_nlev(len0, l, dt);
             }
         }
         __syncwarp();
     }
 
     if (active) {
+        uint32_t tok = 0xffffffffu;
+        if (win != 0x7fffffff) {
+            const int gi = win & 255, grp = win >> 8;
+            const int l = grp / a.M, m = grp % a.M;
+            const int dt = min(a.Dcore, 1 << l);
+            const int is = gi >> 2, q = gi & 3;
+            const int p = (q == 0) ? 0 : (3 * l + q);
+            tok = (uint32_t(m) << 16) | (uint32_t(p) << 8) | uint32_t(is * dt);
+        }
         long o = ((long) b * a.ndm_out + dm) * a.nt_out + tout;
-        ((Ts *) a.out_max)[o] = from_f<Ts>(best.v);
-        a.out_argmax[o] = best.tok;
+        ((Ts *) a.out_max)[o] = from_f<Ts>(best);
+        a.out_argmax[o] = tok;
     }
 }
 
@@ -870,20 +895,33 @@ int pf_warp_floats(int Dout, int tpad, int Dcore, int L)
     return tot;
 }
 
-template<typename Ts>
-static void launch_pf_t(const PfArgs &a, int B, cudaStream_t s)
+template<typename Ts, int L>
+static void launch_pf_l(const PfArgs &a, int B, cudaStream_t s)
 {
     int wf = pf_warp_floats(a.Dout, a.tpad, a.Dcore, a.L);
     size_t sm = (size_t) kPfWarps * wf * sizeof(float);
-    set_smem(pf_kernel<Ts>, sm);
+    set_smem(pf_kernel<Ts, L>, sm);
     dim3 grid((a.nt_out + 31) / 32, (a.ndm_out + kPfWarps - 1) / kPfWarps, B);
-    pf_kernel<Ts><<<grid, kPfWarps * 32, sm, s>>>(a, wf);
+    pf_kernel<Ts, L><<<grid, kPfWarps * 32, sm, s>>>(a, wf);
     check_launch("pf_kernel");
+}
+
+template<typename Ts>
+static void launch_pf_t(const PfArgs &a, int B, cudaStream_t s)
+{
+    switch (a.L) {
+    case 1: launch_pf_l<Ts, 1>(a, B, s); break;
+    case 2: launch_pf_l<Ts, 2>(a, B, s); break;
+    case 3: launch_pf_l<Ts, 3>(a, B, s); break;
+    case 4: launch_pf_l<Ts, 4>(a, B, s); break;
+    case 5: launch_pf_l<Ts, 5>(a, B, s); break;
+    default: throw std::runtime_error("pf_kernel: unsupported number of boxcar levels");
+    }
 }
 
 void launch_pf(const PfArgs &a, int dtype, int B, cudaStream_t s)
 {
-    if (a.L > kPfMaxLevels) throw std::runtime_error("pf_kernel: too many boxcar levels");
+    if (a.Dout > 64 || a.Dout < 1) throw std::runtime_error("pf_kernel: time downsampling must be in [1, 64]");
     if (dtype == 0) launch_pf_t<float>(a, B, s);
     else if (dtype == 1) launch_pf_t<__half>(a, B, s);
     else launch_pf_t<__nv_bfloat16>(a, B, s);
