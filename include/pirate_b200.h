@@ -128,6 +128,24 @@ int pb2_dd_enable_timing(pb2_dedisperser *dd, int on);
 int pb2_dd_kernel_times(pb2_dedisperser *dd, double *ms5, long *counts5);
 void pb2_dd_destroy(pb2_dedisperser *dd);
 
+/* ---- Allocation-free single-chunk dedispersion (no counterpart in pirate) ----
+ *
+ * For callers that cannot allocate device memory, for example a real-time thread that must not
+ * stall on cudaMalloc's device-wide synchronization, or code inside a host framework whose memory
+ * pool must own every device allocation. Dedisperses one chunk of beams_per_batch beams as the first
+ * chunk of a fresh stream (zero history), through the same kernels as the GpuDedisperser, and
+ * allocates nothing: all scratch lives in a static device array of PB2_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until exit. Plans whose scratch exceeds it are rejected.
+ *   in:          device (beams_per_batch, nfreq, nt_in) in the config dtype
+ *   weights[i]:  device (beams_per_batch, ndm_wt, nt_wt, nprofiles, N) float32, per tree
+ *   out_max[i], out_argmax[i]: device (beams_per_batch, ndm_out, nt_out), config dtype / uint32
+ * The array is shared by all calls: calls that overlap on the GPU race and must be serialized.
+ * The first call on a device looks up the array's address (cudaGetSymbolAddress); make that first
+ * call before any stream capture. */
+#define PB2_NOALLOC_SCRATCH_BYTES (32L << 20)
+int pb2_dedisperse_chunk_noalloc(const pb2_plan *plan, const void *in, const float *const *weights,
+                                 void *const *out_max, uint32_t *const *out_argmax, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -279,4 +279,13 @@ int pb2_dd_kernel_times(pb2_dedisperser *dd, double *ms5, long *counts5)
 
 void pb2_dd_destroy(pb2_dedisperser *dd) { delete dd; }
 
+int pb2_dedisperse_chunk_noalloc(const pb2_plan *plan, const void *in, const float *const *weights,
+                                 void *const *out_max, uint32_t *const *out_argmax, void *stream)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(in); REQUIRE_PTR(weights); REQUIRE_PTR(out_max); REQUIRE_PTR(out_argmax);
+        pb2::dedisperse_chunk_noalloc(*plan->p, in, weights, out_max, out_argmax, (cudaStream_t) stream);
+    });
+}
+
 }  // extern "C"

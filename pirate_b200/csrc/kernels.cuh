@@ -126,4 +126,8 @@ void launch_stage1(const Stage1Args &a, int dtype, int nblocks, int B, cudaStrea
 void launch_stage2(const Stage2Args &a, int dtype, int nblocks, int B, cudaStream_t s);
 void launch_pf(const PfArgs &a, int dtype, int B, cudaStream_t s);
 
+struct DedispersionPlan;
+void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, const float *const *weights,
+                              void *const *out_max, uint32_t *const *out_argmax, cudaStream_t stream);
+
 }  // namespace pb2
