@@ -364,6 +364,7 @@ void GpuDedisperser::launch_batch(long seq_id)
             l.cap_mask[p - 1] = s1[p].lds_cap - 1;
         }
         l.state = d_lds_state.as<float>();
+        l.lag_rank = int(plan.stage1_dd_rank[1]);
         l.ichunk = ichunk;
         l.beam0 = beam0; l.B = int(B); l.total_beams = int(total_beams);
         cudaEvent_t t1 = tick(1, nullptr);
@@ -392,8 +393,7 @@ void GpuDedisperser::launch_batch(long seq_id)
             a.in_row_stride = st.lds_cap;
             a.in_mask = st.lds_cap - 1;
             a.in_s0 = ichunk * st.nt;
-            a.in_lag0 = (1 << plan.stage1_dd_rank[p]) - 1;   // lag 2^s1dd - 1 - j (ReferenceLaggedDownsamplingKernel.cpp:53-55)
-            a.in_lag1 = 1;
+            a.in_lag0 = a.in_lag1 = 0;   // the lagged-downsampling kernel wrote the rows already delayed
             a.in_beam0 = beam0;
         }
         a.ring = st.ring.ptr;

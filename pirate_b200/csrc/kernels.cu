@@ -99,7 +99,9 @@ __global__ void __launch_bounds__(256) grid_kernel(GridArgs a)
 // Lagged downsampling. For each level p = 1..nlev:
 //   ds_p[ch][u]  = (ds_{p-1}[ch][2u] + ds_{p-1}[ch][2u+1]) / sqrt2          (ds_0 = level-0 tree)
 //   out_p[c][u]  = (ds_p[2c][u-1] + ds_p[2c+1][u]) / sqrt2                     (one-sample lag on even channels)
-// out_p goes to a per-row delay line; the per-row "large" lag is applied by the stage-1 reader.
+// out_p goes to a per-row delay line, written delayed by the per-row "large" lag
+// 2^s1dd - 1 - (c mod 2^s1dd) (ReferenceLaggedDownsamplingKernel.cpp:53-55), so that the stage-1
+// kernel reads aligned rows.
 // Each thread owns one output row c and a window of W0 level-0 samples.
 
 
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(128) lds_kernel(LdsArgs a)
         long cap = a.cap_mask[p - 1] + 1;
         Ts *ring = (Ts *) a.ring[p - 1] + ((long) bt * nhalf + c) * cap;
         long nt_p = a.T >> p;
-        long s_base = a.ichunk * nt_p + (long) win * len;
+        long s_base = a.ichunk * nt_p + (long) win * len + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
 #pragma unroll
         for (int u = 0; u < (W0 >> 1); u++) {
             if (u < len) {
@@ -246,138 +248,6 @@ __device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP],
             off += L + 1;
         }
 }
-
-// Delay line between the phases, in shared memory: row rr = f * 2^RA + d (f < 2^RB) has capacity
-// P(f, d) + 32; 'pos' is the row's write position for the current tile.
-struct RingTab
-{
-    int *off, *cap, *pos;
-};
-
-template<int RA, int RB>
-__device__ __forceinline__ int ring_lag(int f, int d) { return ((1 << RB) - 1 - f) * brev_bits(d, RA); }
-
-template<int RA, int RB>
-__device__ void ring_init(RingTab &t, int *sm_int, long s0)
-{
-    constexpr int NR = 1 << (RA + RB);
-    t.off = sm_int;
-    t.cap = sm_int + NR;
-    t.pos = sm_int + 2 * NR;
-    if (threadIdx.x == 0) {
-        int o = 0;
-        for (int rr = 0; rr < NR; rr++) {
-            int c = ring_lag<RA, RB>(rr >> RA, rr & ((1 << RA) - 1)) + 32;
-            t.off[rr] = o;
-            t.cap[rr] = c;
-            t.pos[rr] = int(s0 % c);
-            o += c;
-        }
-    }
-}
-
-__device__ __forceinline__ int wrap_add(int p, int cap) { return (p >= cap) ? (p - cap) : ((p < 0) ? (p + cap) : p); }
-
-template<typename Ts, int RA, int RB>
-__global__ void __launch_bounds__(tree_threads(RA + RB)) stage1_kernel(Stage1Args a)
-{
-    constexpr int NA = 1 << RA, NB = 1 << RB, NR = 1 << (RA + RB);
-    constexpr int RING = ring_floats(RA, RB);
-    extern __shared__ long long sm_ll[];
-    int *sm_int = (int *) sm_ll;
-    RingTab tab;
-    int *opos = sm_int + 3 * NR;                    // output delay-line write positions, by final row
-    float *ring = (float *) (sm_int + 4 * NR);
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
-    float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
-    const Ts *in = (const Ts *) a.in + (long) (a.in_beam0 + b) * a.in_beam_stride;
-    Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride;
-    const long *out_off = a.ring_off + (long) blk * NR;
-    const int *out_cap = a.ring_cap + (long) blk * NR;
-
-    ring_init<RA, RB>(tab, sm_int, a.s0);
-    for (int i = threadIdx.x; i < NR; i += blockDim.x)
-        opos[i] = int(a.s0 % out_cap[i]);
-    for (int i = threadIdx.x; i < RING; i += blockDim.x)
-        ring[i] = st[i];
-
-    const bool in_a = warp < NB, in_b = warp < NA;
-    float pva[RT<RA>::NS][RT<RA>::NP], pvb[RT<RB>::NS][RT<RB>::NP];
-    const float *sta = st + RING + warp * rt_state(RA);
-    const float *stb = st + RING + NB * rt_state(RA) + warp * rt_state(RB);
-    if (in_a) rt_load<RA>(pva, sta, lane);
-    if (in_b) rt_load<RB>(pvb, stb, lane);
-    __syncthreads();
-
-    // Phase-a input rows c = blk*NR + warp*NA + i, lag(c) = in_lag0 - in_lag1*(warp*NA + i).
-    const long rowbase = ((long) blk * NR + warp * NA) * a.in_row_stride;
-    float nxt[NA];
-    if (in_a) {
-#pragma unroll
-        for (int i = 0; i < NA; i++) {
-            int lag = a.in_lag0 - a.in_lag1 * (warp * NA + i);
-            nxt[i] = to_f(in[rowbase + i * a.in_row_stride + ((a.in_s0 + lane - lag) & a.in_mask)]);
-        }
-    }
-
-    const int ntiles = a.nt / 32;
-    for (int tile = 0; tile < ntiles; tile++) {
-        if (in_a) {
-            float v[NA];
-#pragma unroll
-            for (int i = 0; i < NA; i++) v[i] = nxt[i];
-            if (tile + 1 < ntiles) {
-                long s_in = a.in_s0 + (long) (tile + 1) * 32 + lane;
-#pragma unroll
-                for (int i = 0; i < NA; i++) {
-                    int lag = a.in_lag0 - a.in_lag1 * (warp * NA + i);
-                    nxt[i] = to_f(in[rowbase + i * a.in_row_stride + ((s_in - lag) & a.in_mask)]);
-                }
-            }
-            rt_steps<RA>(v, pva, lane);
-#pragma unroll
-            for (int i = 0; i < NA; i++) {
-                int rr = warp * NA + i;
-                ring[tab.off[rr] + wrap_add(tab.pos[rr] + lane, tab.cap[rr])] = v[i];
-            }
-        }
-        __syncthreads();
-        if (in_b) {
-            float v[NB];
-#pragma unroll
-            for (int f = 0; f < NB; f++) {
-                int rr = f * NA + warp;
-                int p = tab.pos[rr] + lane - ring_lag<RA, RB>(f, warp);
-                v[f] = ring[tab.off[rr] + wrap_add(p, tab.cap[rr])];
-            }
-            __syncwarp();
-            if (lane < NB) {
-                int rr = lane * NA + warp;
-                tab.pos[rr] = wrap_add(tab.pos[rr] + 32, tab.cap[rr]);
-            }
-            rt_steps<RB>(v, pvb, lane);
-#pragma unroll
-            for (int f = 0; f < NB; f++) {
-                int i = (f << RA) | warp;
-                out[out_off[i] + wrap_add(opos[i] + lane, out_cap[i])] = from_f<Ts>(v[f]);
-            }
-            __syncwarp();
-            if (lane < NB) {
-                int i = (lane << RA) | warp;
-                opos[i] = wrap_add(opos[i] + 32, out_cap[i]);
-            }
-        }
-        __syncthreads();
-    }
-
-    for (int i = threadIdx.x; i < RING; i += blockDim.x)
-        st[i] = ring[i];
-    if (in_a) rt_save<RA>(pva, (float *) sta, lane);
-    if (in_b) rt_save<RB>(pvb, (float *) stb, lane);
-}
-
 
 // Phase b of a stage-2 (subband) tree: before step r' (r' = 0..RB-1) and after it, subband rows of
 // pf level r'+1 are emitted (FrequencySubbands multiplet order), reproducing ReferenceTree::dedisperse_2d
@@ -480,116 +350,251 @@ struct PfEmit
     }
 };
 
-template<typename Ts, int RA, int RB, bool STAG>
-__global__ void __launch_bounds__(tree_threads(RA + RB)) stage2_kernel(Stage2Args a)
+// Shared-memory delay line between the phases: row rr = f * 2^RA + d (f < 2^RB) has capacity
+// P(f, d) + 64. Phase a writes tile k at wpos while phase b reads tile k-1 at rpos - P.
+struct RingTab
+{
+    int *off, *cap, *wpos, *rpos;
+};
+
+template<int RA, int RB>
+__device__ __forceinline__ int ring_lag(int f, int d) { return ((1 << RB) - 1 - f) * brev_bits(d, RA); }
+
+__device__ __forceinline__ int wrap_add(int p, int cap) { return (p >= cap) ? (p - cap) : ((p < 0) ? (p + cap) : p); }
+
+template<int RA, int RB>
+__device__ void ring_init(RingTab &t, int *sm_int, long s0)
+{
+    constexpr int NR = 1 << (RA + RB);
+    t.off = sm_int;
+    t.cap = sm_int + NR;
+    t.wpos = sm_int + 2 * NR;
+    t.rpos = sm_int + 3 * NR;
+    if (threadIdx.x == 0) {
+        int o = 0;
+        for (int rr = 0; rr < NR; rr++) {
+            int c = ring_lag<RA, RB>(rr >> RA, rr & ((1 << RA) - 1)) + 64;
+            t.off[rr] = o;
+            t.cap[rr] = c;
+            t.wpos[rr] = t.rpos[rr] = int(s0 % c);
+            o += c;
+        }
+    }
+}
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    unsigned s = (unsigned) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" :: "r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Staging of one tile of a phase-a warp's NA input rows: 32-bit words copied with cp.async.
+// float: 32 words per row; 16-bit types: 17 words (34 samples) starting at an even sample.
+template<typename Ts> struct Stage
+{
+    static constexpr int WPR = (sizeof(Ts) == 4) ? 32 : 17;   // words per row
+    static constexpr int SPR = (sizeof(Ts) == 4) ? 32 : 34;   // samples per row
+};
+
+template<int STAGE>
+struct TreeArgsOf;
+template<> struct TreeArgsOf<1> { using type = Stage1Args; };
+template<> struct TreeArgsOf<2> { using type = Stage2Args; };
+
+// Two-phase tree kernel. Warps [0, NB) run phase a on tile k while warps [NB, NB+NA) run phase b on
+// tile k-1; one block barrier per tile.
+//   STAGE 1: input = level-p tree rows (aligned), output = per-row stage-1 delay lines.
+//   STAGE 2: input = stage-1 delay lines read at lag rb_lag (misaligned), output = subband rows.
+template<typename Ts, int RA, int RB, int STAGE, bool STAG>
+__global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(typename TreeArgsOf<STAGE>::type a)
 {
     constexpr int NA = 1 << RA, NB = 1 << RB, NR = 1 << (RA + RB);
     constexpr int RING = ring_floats(RA, RB);
+    // Stage-1 rows are read aligned (32 samples = 16 words for 16-bit storage); stage-2 rows start at
+    // an arbitrary sample and need one extra word. Copying the extra word for aligned rows would read
+    // past the end of the last row's buffer.
+    constexpr int WPR = (STAGE == 1 && sizeof(Ts) != 4) ? 16 : Stage<Ts>::WPR;
+    constexpr int SPR = Stage<Ts>::SPR;
     extern __shared__ long long sm_ll[];
-    long *ioff = (long *) sm_ll;                    // offset of the input delay line of row a
-    int *sm_int = (int *) (ioff + NR);
+
+    // Shared layout: [in_off (NR longs) | ring tables 4*NR ints | in_pos, in_cap, out_pos NR ints each |
+    //                 staging 2 x NB x NA x SPR | ring RING floats]
+    long *in_off = (long *) sm_ll;
+    int *sm_int = (int *) (in_off + NR);
     RingTab tab;
-    int *ipos = sm_int + 3 * NR;                    // its next read position
-    int *icap = ipos + NR;                          // its capacity
-    float *ring = (float *) (icap + NR);
+    int *in_pos = sm_int + 4 * NR;
+    int *in_cap = in_pos + NR;
+    int *out_pos = in_cap + NR;
+    Ts *staging = (Ts *) (out_pos + NR);
+    float *ring = (float *) (staging + 2 * NB * NA * SPR);
+    ring = (float *) (((uintptr_t) ring + 15) & ~uintptr_t(15));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int d = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
-    float *st = a.state + ((long) bt * gridDim.x + d) * a.state_per_block;
-    const Ts *in = (const Ts *) a.ring + (long) bt * a.ring_beam_stride;
+    const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
+    float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
 
     ring_init<RA, RB>(tab, sm_int, a.s0);
-    const long dm1 = brev_bits(d, a.amb_rank) + (a.uflag ? (1L << a.amb_rank) : 0L);
-    for (int r = threadIdx.x; r < NR; r += blockDim.x) {
-        long row = ((long) r << a.amb_rank) + d;
-        long lag = (long) (NR - 1 - r) * dm1;
-        long cap = a.ring_cap[row];
-        long p = (a.s0 - lag) % cap;
-        ipos[r] = int(p < 0 ? p + cap : p);
-        icap[r] = int(cap);
-        ioff[r] = a.ring_off[row];
-    }
     for (int i = threadIdx.x; i < RING; i += blockDim.x)
         ring[i] = st[i];
 
-    const bool in_a = warp < NB, in_b = warp < NA;
-    float pva[RT<RA>::NS][RT<RA>::NP], pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
-    const float *sta = st + RING + warp * rt_state(RA);
-    const float *stb = st + RING + NB * rt_state(RA) + warp * (rt_state(RB) + st_state(RB));
-    if (in_a) rt_load<RA>(pva, sta, lane);
-    if (in_b) {
+    const Ts *in;
+    if constexpr (STAGE == 1) {
+        in = (const Ts *) a.in + (long) (a.in_beam0 + b) * a.in_beam_stride;
+        for (int r = threadIdx.x; r < NR; r += blockDim.x) {
+            in_off[r] = ((long) blk * NR + r) * a.in_row_stride;
+            in_pos[r] = int(a.in_s0 & a.in_mask);
+            in_cap[r] = int(a.in_mask + 1);   // unused for plain rows (mask = -1)
+            out_pos[r] = int(a.s0 % a.ring_cap[(long) blk * NR + r]);
+        }
+    } else {
+        in = (const Ts *) a.ring + (long) bt * a.ring_beam_stride;
+        const long dm1 = brev_bits(blk, a.amb_rank) + (a.uflag ? (1L << a.amb_rank) : 0L);
+        for (int r = threadIdx.x; r < NR; r += blockDim.x) {
+            long row = ((long) r << a.amb_rank) + blk;
+            long lag = (long) (NR - 1 - r) * dm1;
+            long cap = a.ring_cap[row];
+            long p = (a.s0 - lag) % cap;
+            in_pos[r] = int(p < 0 ? p + cap : p);
+            in_cap[r] = int(cap);
+            in_off[r] = a.ring_off[row];
+        }
+    }
+
+    const bool is_a = warp < NB;
+    const int g = is_a ? warp : (warp - NB);   // phase-a group (f) or phase-b group (d)
+    const int ntiles = a.nt / 32;
+    __syncthreads();
+
+    // The two warp roles run separate loops (so each holds only its own histories in registers);
+    // they meet once per tile at named barrier 1.
+    if (is_a) {
+        float pva[RT<RA>::NS][RT<RA>::NP];
+        float *sta = st + RING + g * rt_state(RA);
+        rt_load<RA>(pva, sta, lane);
+
+        // Issues the cp.async copies of this warp's NA rows for one tile into staging buffer 'buf',
+        // then advances the rows' read positions by 32 samples.
+        Ts *my_stage = staging + g * NA * SPR;
+        auto issue = [&](int buf) {
+            Ts *dst = my_stage + buf * NB * NA * SPR;
+            for (int idx = lane; idx < NA * WPR; idx += 32) {
+                const int i = idx / WPR, w = idx - i * WPR;
+                const int r = g * NA + i;
+                int p = in_pos[r];
+                const Ts *src;
+                if constexpr (STAGE == 1) {
+                    src = in + in_off[r] + ((sizeof(Ts) == 4) ? (p + w) : (p + 2 * w));
+                } else {
+                    int c = in_cap[r];
+                    int q = (sizeof(Ts) == 4) ? wrap_add(p + w, c) : wrap_add((p & ~1) + 2 * w, c);
+                    src = in + in_off[r] + q;
+                }
+                cp_async4(dst + i * SPR + ((sizeof(Ts) == 4) ? w : 2 * w), src);
+            }
+            __syncwarp();
+            if (lane < NA) {
+                const int r = g * NA + lane;
+                if constexpr (STAGE == 1) in_pos[r] = int((in_pos[r] + 32) & a.in_mask);
+                else in_pos[r] = wrap_add(in_pos[r] + 32, in_cap[r]);
+            }
+            __syncwarp();
+        };
+
+        unsigned par = 0;   // stage 2, 16-bit storage: bit i = sample parity of row i (constant: capacities are even)
+        if (STAGE == 2 && sizeof(Ts) != 4) {
+#pragma unroll
+            for (int i = 0; i < NA; i++) par |= unsigned(in_pos[g * NA + i] & 1) << i;
+        }
+        issue(0);
+        cp_async_commit();
+
+        for (int it = 0; it <= ntiles; it++) {
+            if (it < ntiles) {
+                if (it + 1 < ntiles) issue((it + 1) & 1);
+                cp_async_commit();
+                cp_async_wait1();
+                __syncwarp();
+                const Ts *sb = my_stage + (it & 1) * NB * NA * SPR;
+                float v[NA];
+#pragma unroll
+                for (int i = 0; i < NA; i++) v[i] = to_f(sb[i * SPR + lane + ((par >> i) & 1)]);
+                rt_steps<RA>(v, pva, lane);
+#pragma unroll
+                for (int i = 0; i < NA; i++) {
+                    const int rr = g * NA + i;
+                    ring[tab.off[rr] + wrap_add(tab.wpos[rr] + lane, tab.cap[rr])] = v[i];
+                }
+                __syncwarp();
+                if (lane < NA) {
+                    const int rr = g * NA + lane;
+                    tab.wpos[rr] = wrap_add(tab.wpos[rr] + 32, tab.cap[rr]);
+                }
+            }
+            asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
+        }
+        cp_async_wait0();
+        rt_save<RA>(pva, sta, lane);
+    } else {
+        float pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
+        float *stb = st + RING + NB * rt_state(RA) + g * (rt_state(RB) + (STAGE == 2 ? st_state(RB) : 0));
         rt_load<RB>(pvb, stb, lane);
         if (STAG) st_load<RB>(psb, stb + rt_state(RB), lane);
+
+        PfEmit<Ts> emit;
+        if constexpr (STAGE == 2) {
+            emit.pf = (Ts *) a.pf;
+            emit.cap = a.pf_cap;
+            emit.mask = a.pf_cap - 1;
+            const int pf_dm = brev_bits(g, RA);
+            emit.rowbase = ((long) bt * a.ndm_out + ((long) brev_bits(blk, a.amb_rank) << RA) + pf_dm) * a.M;
+        }
+
+        for (int it = 0; it <= ntiles; it++) {
+            if (it >= 1) {
+                const int tile = it - 1;
+                float v[NB];
+#pragma unroll
+                for (int f = 0; f < NB; f++) {
+                    const int rr = f * NA + g;
+                    v[f] = ring[tab.off[rr] + wrap_add(tab.rpos[rr] + lane - ring_lag<RA, RB>(f, g), tab.cap[rr])];
+                }
+                __syncwarp();
+                if (lane < NB) {
+                    const int rr = lane * NA + g;
+                    tab.rpos[rr] = wrap_add(tab.rpos[rr] + 32, tab.cap[rr]);
+                }
+                if constexpr (STAGE == 1) {
+                    rt_steps<RB>(v, pvb, lane);
+                    Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride;
+                    const long *oo = a.ring_off + (long) blk * NR;
+                    const int *oc = a.ring_cap + (long) blk * NR;
+#pragma unroll
+                    for (int f = 0; f < NB; f++) {
+                        const int i = (f << RA) | g;
+                        out[oo[i] + wrap_add(out_pos[i] + lane, oc[i])] = from_f<Ts>(v[f]);
+                    }
+                    __syncwarp();
+                    if (lane < NB) {
+                        const int i = (lane << RA) | g;
+                        out_pos[i] = wrap_add(out_pos[i] + 32, oc[i]);
+                    }
+                } else {
+                    emit.s = a.s0 + (long) tile * 32 + lane;
+                    phase_b_subbands<RB, STAG>(v, pvb, psb, a, lane, emit);
+                }
+            }
+            asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
+        }
+        rt_save<RB>(pvb, stb, lane);
+        if (STAG) st_save<RB>(psb, stb + rt_state(RB), lane);
     }
     __syncthreads();
 
-    float nxt[NA];
-    if (in_a) {
-#pragma unroll
-        for (int i = 0; i < NA; i++) {
-            int r = warp * NA + i;
-            nxt[i] = to_f(in[ioff[r] + wrap_add(ipos[r] + lane, icap[r])]);
-        }
-    }
-
-    PfEmit<Ts> emit;
-    emit.pf = (Ts *) a.pf;
-    emit.cap = a.pf_cap;
-    emit.mask = a.pf_cap - 1;
-    const int pf_dm = brev_bits(warp, RA);
-    emit.rowbase = ((long) bt * a.ndm_out + ((long) brev_bits(d, a.amb_rank) << RA) + pf_dm) * a.M;
-
-    const int ntiles = a.nt / 32;
-    for (int tile = 0; tile < ntiles; tile++) {
-        if (in_a) {
-            float v[NA];
-#pragma unroll
-            for (int i = 0; i < NA; i++) v[i] = nxt[i];
-            if (tile + 1 < ntiles) {
-#pragma unroll
-                for (int i = 0; i < NA; i++) {
-                    int r = warp * NA + i;
-                    int c = icap[r];
-                    int p = wrap_add(ipos[r] + 32, c);
-                    nxt[i] = to_f(in[ioff[r] + wrap_add(p + lane, c)]);
-                    __syncwarp();
-                    if (lane == 0) ipos[r] = p;
-                }
-            }
-            rt_steps<RA>(v, pva, lane);
-#pragma unroll
-            for (int i = 0; i < NA; i++) {
-                int rr = warp * NA + i;
-                ring[tab.off[rr] + wrap_add(tab.pos[rr] + lane, tab.cap[rr])] = v[i];
-            }
-        }
-        __syncthreads();
-        if (in_b) {
-            float v[NB];
-#pragma unroll
-            for (int f = 0; f < NB; f++) {
-                int rr = f * NA + warp;
-                int p = tab.pos[rr] + lane - ring_lag<RA, RB>(f, warp);
-                v[f] = ring[tab.off[rr] + wrap_add(p, tab.cap[rr])];
-            }
-            __syncwarp();
-            if (lane < NB) {
-                int rr = lane * NA + warp;
-                tab.pos[rr] = wrap_add(tab.pos[rr] + 32, tab.cap[rr]);
-            }
-            emit.s = a.s0 + (long) tile * 32 + lane;
-            phase_b_subbands<RB, STAG>(v, pvb, psb, a, lane, emit);
-        }
-        __syncthreads();
-    }
-
     for (int i = threadIdx.x; i < RING; i += blockDim.x)
         st[i] = ring[i];
-    if (in_a) rt_save<RA>(pva, (float *) sta, lane);
-    if (in_b) {
-        rt_save<RB>(pvb, (float *) stb, lane);
-        if (STAG) st_save<RB>(psb, (float *) stb + rt_state(RB), lane);
-    }
 }
 
 
@@ -802,8 +807,13 @@ void launch_lds(const LdsArgs &a, int dtype, cudaStream_t s)
     else launch_lds_d<__nv_bfloat16>(a, s);
 }
 
-template<int RA, int RB>
-static size_t tree_smem() { return (size_t) ring_floats(RA, RB) * sizeof(float) + 8 * (1 << (RA + RB)) * sizeof(int); }
+template<typename Ts, int RA, int RB>
+static size_t tree_smem()
+{
+    constexpr int NR = 1 << (RA + RB);
+    return (size_t) NR * 8 + 7 * NR * 4 + 2 * (1 << RB) * (1 << RA) * Stage<Ts>::SPR * sizeof(Ts) + 16
+           + (size_t) ring_floats(RA, RB) * sizeof(float);
+}
 
 template<typename K>
 static void set_smem(K kernel, size_t bytes)
@@ -812,77 +822,53 @@ static void set_smem(K kernel, size_t bytes)
     if (e != cudaSuccess) throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
 }
 
-template<typename Ts, int R>
-static void launch_stage1_r(const Stage1Args &a, int nblocks, int B, cudaStream_t s)
+template<typename Ts, int R, int STAGE, bool STAG, typename A>
+static void launch_tree_r(const A &a, int nblocks, int B, cudaStream_t s)
 {
     constexpr int RA = split_ra(R), RB = split_rb(R);
-    size_t sm = tree_smem<RA, RB>();
-    set_smem(stage1_kernel<Ts, RA, RB>, sm);
-    stage1_kernel<Ts, RA, RB><<<dim3(nblocks, B), tree_threads(R), sm, s>>>(a);
-    check_launch("stage1_kernel");
+    size_t sm = tree_smem<Ts, RA, RB>();
+    set_smem(tree_kernel<Ts, RA, RB, STAGE, STAG>, sm);
+    tree_kernel<Ts, RA, RB, STAGE, STAG><<<dim3(nblocks, B), tree_threads(R), sm, s>>>(a);
+    check_launch(STAGE == 1 ? "stage1 tree_kernel" : "stage2 tree_kernel");
 }
 
-template<typename Ts>
-static void launch_stage1_t(const Stage1Args &a, int nblocks, int B, cudaStream_t s)
+template<typename Ts, int STAGE, bool STAG, typename A>
+static void launch_tree_t(const A &a, int nblocks, int B, cudaStream_t s)
 {
     switch (a.rank) {
-    case 1: launch_stage1_r<Ts, 1>(a, nblocks, B, s); break;
-    case 2: launch_stage1_r<Ts, 2>(a, nblocks, B, s); break;
-    case 3: launch_stage1_r<Ts, 3>(a, nblocks, B, s); break;
-    case 4: launch_stage1_r<Ts, 4>(a, nblocks, B, s); break;
-    case 5: launch_stage1_r<Ts, 5>(a, nblocks, B, s); break;
-    case 6: launch_stage1_r<Ts, 6>(a, nblocks, B, s); break;
-    case 7: launch_stage1_r<Ts, 7>(a, nblocks, B, s); break;
-    case 8: launch_stage1_r<Ts, 8>(a, nblocks, B, s); break;
-    default: throw std::runtime_error("stage1_kernel: unsupported dd rank " + std::to_string(a.rank));
+    case 1: launch_tree_r<Ts, 1, STAGE, STAG>(a, nblocks, B, s); break;
+    case 2: launch_tree_r<Ts, 2, STAGE, STAG>(a, nblocks, B, s); break;
+    case 3: launch_tree_r<Ts, 3, STAGE, STAG>(a, nblocks, B, s); break;
+    case 4: launch_tree_r<Ts, 4, STAGE, STAG>(a, nblocks, B, s); break;
+    case 5: launch_tree_r<Ts, 5, STAGE, STAG>(a, nblocks, B, s); break;
+    case 6: launch_tree_r<Ts, 6, STAGE, STAG>(a, nblocks, B, s); break;
+    case 7: launch_tree_r<Ts, 7, STAGE, STAG>(a, nblocks, B, s); break;
+    case 8: launch_tree_r<Ts, 8, STAGE, STAG>(a, nblocks, B, s); break;
+    default: throw std::runtime_error("tree_kernel: unsupported dd rank " + std::to_string(a.rank));
     }
 }
 
 void launch_stage1(const Stage1Args &a, int dtype, int nblocks, int B, cudaStream_t s)
 {
-    if (dtype == 0) launch_stage1_t<float>(a, nblocks, B, s);
-    else if (dtype == 1) launch_stage1_t<__half>(a, nblocks, B, s);
-    else launch_stage1_t<__nv_bfloat16>(a, nblocks, B, s);
-}
-
-template<typename Ts, int R>
-static void launch_stage2_r(const Stage2Args &a, int nblocks, int B, cudaStream_t s)
-{
-    constexpr int RA = split_ra(R), RB = split_rb(R);
-    size_t sm = tree_smem<RA, RB>();
-    bool stag = false;
-    for (int l = 1; l <= RB; l++) stag = stag || (a.sb_count[l] >= 2);
-    if (stag) {
-        set_smem(stage2_kernel<Ts, RA, RB, true>, sm);
-        stage2_kernel<Ts, RA, RB, true><<<dim3(nblocks, B), tree_threads(R), sm, s>>>(a);
-    } else {
-        set_smem(stage2_kernel<Ts, RA, RB, false>, sm);
-        stage2_kernel<Ts, RA, RB, false><<<dim3(nblocks, B), tree_threads(R), sm, s>>>(a);
-    }
-    check_launch("stage2_kernel");
-}
-
-template<typename Ts>
-static void launch_stage2_t(const Stage2Args &a, int nblocks, int B, cudaStream_t s)
-{
-    switch (a.rank) {
-    case 1: launch_stage2_r<Ts, 1>(a, nblocks, B, s); break;
-    case 2: launch_stage2_r<Ts, 2>(a, nblocks, B, s); break;
-    case 3: launch_stage2_r<Ts, 3>(a, nblocks, B, s); break;
-    case 4: launch_stage2_r<Ts, 4>(a, nblocks, B, s); break;
-    case 5: launch_stage2_r<Ts, 5>(a, nblocks, B, s); break;
-    case 6: launch_stage2_r<Ts, 6>(a, nblocks, B, s); break;
-    case 7: launch_stage2_r<Ts, 7>(a, nblocks, B, s); break;
-    case 8: launch_stage2_r<Ts, 8>(a, nblocks, B, s); break;
-    default: throw std::runtime_error("stage2_kernel: unsupported dd rank " + std::to_string(a.rank));
-    }
+    if (a.in_lag0 != 0 || a.in_lag1 != 0) throw std::runtime_error("launch_stage1: input rows must be aligned (no read lag)");
+    if (dtype == 0) launch_tree_t<float, 1, false>(a, nblocks, B, s);
+    else if (dtype == 1) launch_tree_t<__half, 1, false>(a, nblocks, B, s);
+    else launch_tree_t<__nv_bfloat16, 1, false>(a, nblocks, B, s);
 }
 
 void launch_stage2(const Stage2Args &a, int dtype, int nblocks, int B, cudaStream_t s)
 {
-    if (dtype == 0) launch_stage2_t<float>(a, nblocks, B, s);
-    else if (dtype == 1) launch_stage2_t<__half>(a, nblocks, B, s);
-    else launch_stage2_t<__nv_bfloat16>(a, nblocks, B, s);
+    bool stag = false;
+    for (int l = 1; l < 5; l++) stag = stag || (a.sb_count[l] >= 2);
+    if (stag) {
+        if (dtype == 0) launch_tree_t<float, 2, true>(a, nblocks, B, s);
+        else if (dtype == 1) launch_tree_t<__half, 2, true>(a, nblocks, B, s);
+        else launch_tree_t<__nv_bfloat16, 2, true>(a, nblocks, B, s);
+    } else {
+        if (dtype == 0) launch_tree_t<float, 2, false>(a, nblocks, B, s);
+        else if (dtype == 1) launch_tree_t<__half, 2, false>(a, nblocks, B, s);
+        else launch_tree_t<__nv_bfloat16, 2, false>(a, nblocks, B, s);
+    }
 }
 
 int pf_warp_floats(int Dout, int tpad, int Dcore, int L)

@@ -14,10 +14,11 @@ namespace pb2 {
 __host__ __device__ constexpr int split_rb(int R) { return (R + 1) / 2; }
 __host__ __device__ constexpr int split_ra(int R) { return R - (R + 1) / 2; }
 
-// Threads per block of a two-phase tree kernel of rank R (one warp per register-tree group).
+// Threads per block of a two-phase tree kernel of rank R: one warp per phase-a group (2^RB of
+// them) followed by one warp per phase-b group (2^RA).
 __host__ __device__ constexpr int tree_threads(int R)
 {
-    return 32 * ((split_ra(R) > split_rb(R)) ? (1 << split_ra(R)) : (1 << split_rb(R)));
+    return 32 * ((1 << split_ra(R)) + (1 << split_rb(R)));
 }
 
 // Stage 1 (one primary tree): input rows -> two-phase tree -> per-row output delay lines.
@@ -27,8 +28,8 @@ struct Stage1Args
     long state_per_block;   // floats
     float *state;           // (total_beams, nblocks, state_per_block)
 
-    // Input element (b, row c, time s) at in + (in_beam0 + b)*in_beam_stride + c*in_row_stride + ((s - lag(c)) & in_mask),
-    // lag(c) = in_lag0 - in_lag1 * (c mod 2^rank).
+    // Input element (b, row c, time s) at in + (in_beam0 + b)*in_beam_stride + c*in_row_stride + (s & in_mask),
+    // (in_lag0 and in_lag1 must be zero: rows are read aligned).
     const void *in;
     long in_beam_stride, in_row_stride, in_mask;
     long in_s0;             // time of the chunk's first sample in the input's indexing
@@ -112,6 +113,7 @@ struct LdsArgs
     void *ring[6];          // per level p=1..nlev: delay lines (total_beams, 2^(rank-1), cap[p])
     long cap_mask[6];
     float *state;           // (2, total_beams, nlev, 2^(rank-1)) last even-channel sample per level
+    int lag_rank;           // output row c is written delayed by 2^lag_rank - 1 - (c mod 2^lag_rank) samples
     long ichunk;
     int beam0, B, total_beams;
 };

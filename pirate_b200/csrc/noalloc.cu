@@ -202,6 +202,7 @@ void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, cons
         l.rank = int(rank); l.T = int(nt); l.nlev = int(npri - 1);
         for (long p = 1; p < npri; p++) { l.ring[p - 1] = P(s1[p].lds); l.cap_mask[p - 1] = s1[p].lds_cap - 1; }
         l.state = (float *) P(lds_state);
+        l.lag_rank = int(plan.stage1_dd_rank[1]);
         l.ichunk = 0;
         l.beam0 = 0; l.B = int(B); l.total_beams = int(B);
         launch_lds(l, dtype_code, stream);
@@ -218,7 +219,7 @@ void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, cons
             a.in = P(tree0); a.in_beam_stride = N * nt; a.in_row_stride = nt; a.in_mask = -1;
         } else {
             a.in = P(st.lds); a.in_beam_stride = (N / 2) * st.lds_cap; a.in_row_stride = st.lds_cap;
-            a.in_mask = st.lds_cap - 1; a.in_lag0 = (1 << st.rank) - 1; a.in_lag1 = 1;
+            a.in_mask = st.lds_cap - 1; a.in_s0 = 0;
         }
         a.ring = P(st.ring);
         a.ring_off = (const long *) T(st.ring_off_t);

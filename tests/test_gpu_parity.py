@@ -87,3 +87,21 @@ def test_lowp_vs_fp64(pb2lib, dtype, case, tol):
     for i in range(orc.ntrees):
         ev = orc64.eval_tokens(i, gres[last][1][i], ws[i][0])
         assert np.abs(ev - ores[last][0][i]).max() <= 2 * tol
+
+
+def test_fp32_bitwise_rank16(pb2lib):
+    """Maximum tree rank (16): stage ranks 8+8 (the 4+4 register-tree split) and buffers whose sizes
+    end on page boundaries; two chunks bitwise against the fp32 oracle."""
+    prim = [dict(num_early_triggers=1, max_width=32, dm_downsampling=0, time_downsampling=0,
+                 wt_dm_downsampling=64, wt_time_downsampling=64)]
+    cfg = H.toy_config(rank=16, nfreq=4096, nt=2048, dtype="float32", subbands=[0, 2, 0, 0, 1],
+                       beams_per_gpu=1, beams_per_batch=1, primary_trees=prim)
+    xs = H.make_inputs(cfg, 2, seed=16)
+    orc, _ = H.run_oracle(cfg, xs[:0], [])
+    ws = H.make_weights(orc, seed=16)
+    _, ores = H.run_oracle(cfg, xs, ws, 1, 32)
+    _, _, gres = H.run_gpu(pb2lib, cfg, xs, ws)
+    for seq in range(len(xs)):
+        for i in range(orc.ntrees):
+            assert np.array_equal(gres[seq][0][i], ores[seq][0][i]), "seq %d tree %d out_max" % (seq, i)
+            assert np.array_equal(gres[seq][1][i], ores[seq][1][i]), "seq %d tree %d out_argmax" % (seq, i)
