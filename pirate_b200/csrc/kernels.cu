@@ -423,7 +423,8 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     // Shared layout: [in_off (NR longs) | ring tables 4*NR ints | in_pos, in_cap, out_pos NR ints each |
     //                 staging 2 x NB x NA x SPR | ring RING floats]
     long *in_off = (long *) sm_ll;
-    int *sm_int = (int *) (in_off + NR);
+    long *out_off = in_off + NR;                    // stage 1: offsets of the output delay lines
+    int *sm_int = (int *) (out_off + NR);
     RingTab tab;
     int *in_pos = sm_int + 4 * NR;
     int *in_cap = in_pos + NR;
@@ -446,8 +447,9 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
         for (int r = threadIdx.x; r < NR; r += blockDim.x) {
             in_off[r] = ((long) blk * NR + r) * a.in_row_stride;
             in_pos[r] = int(a.in_s0 & a.in_mask);
-            in_cap[r] = int(a.in_mask + 1);   // unused for plain rows (mask = -1)
-            out_pos[r] = int(a.s0 % a.ring_cap[(long) blk * NR + r]);
+            in_cap[r] = a.ring_cap[(long) blk * NR + r];   // stage 1: capacity of output delay line r
+            out_off[r] = a.ring_off[(long) blk * NR + r];
+            out_pos[r] = int(a.s0 % in_cap[r]);
         }
     } else {
         in = (const Ts *) a.ring + (long) bt * a.ring_beam_stride;
@@ -569,17 +571,15 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 if constexpr (STAGE == 1) {
                     rt_steps<RB>(v, pvb, lane);
                     Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride;
-                    const long *oo = a.ring_off + (long) blk * NR;
-                    const int *oc = a.ring_cap + (long) blk * NR;
 #pragma unroll
                     for (int f = 0; f < NB; f++) {
                         const int i = (f << RA) | g;
-                        out[oo[i] + wrap_add(out_pos[i] + lane, oc[i])] = from_f<Ts>(v[f]);
+                        out[out_off[i] + wrap_add(out_pos[i] + lane, in_cap[i])] = from_f<Ts>(v[f]);
                     }
                     __syncwarp();
                     if (lane < NB) {
                         const int i = (lane << RA) | g;
-                        out_pos[i] = wrap_add(out_pos[i] + 32, oc[i]);
+                        out_pos[i] = wrap_add(out_pos[i] + 32, in_cap[i]);
                     }
                 } else {
                     emit.s = a.s0 + (long) tile * 32 + lane;
@@ -811,7 +811,7 @@ template<typename Ts, int RA, int RB>
 static size_t tree_smem()
 {
     constexpr int NR = 1 << (RA + RB);
-    return (size_t) NR * 8 + 7 * NR * 4 + 2 * (1 << RB) * (1 << RA) * Stage<Ts>::SPR * sizeof(Ts) + 16
+    return (size_t) 2 * NR * 8 + 7 * NR * 4 + 2 * (1 << RB) * (1 << RA) * Stage<Ts>::SPR * sizeof(Ts) + 16
            + (size_t) ring_floats(RA, RB) * sizeof(float);
 }
 
