@@ -334,7 +334,7 @@ def main():
     value = nbeams_total * CHUNK_SECONDS / (r["ms_per_step"] * 1e-3)
     e2e = nbeams_total * CHUNK_SECONDS / (r["e2e_ms_per_step"] * 1e-3)
 
-    classes = ["grid", "lds", "stage1", "stage2", "pf"]
+    classes = ["grid_lds", "unused", "stage1", "stage2", "pf"]
     kt = r["ktimes"]
     tot_ms = sum(kt[c][0] for c in classes)
     dom = max(classes, key=lambda c: kt[c][0])

@@ -118,12 +118,12 @@ int pb2_dd_fill_weights(pb2_dedisperser *dd, long itree, const float *host, long
 /* GpuDedisperser::stop, src_lib/GpuDedisperser.cpp:735 */
 int pb2_dd_stop(pb2_dedisperser *dd);
 /* Kernel launches per (chunk, batch), and algorithmic HBM bytes per (chunk, batch) for the
- * kernel classes [grid, lds, stage1, stage2, pf]. */
+ * kernel classes [grid+lds (one fused kernel), unused, stage1, stage2, pf]. */
 int pb2_dd_kernels_per_batch(const pb2_dedisperser *dd, long *n);
 int pb2_dd_algorithmic_bytes(const pb2_dedisperser *dd, double *out5);
 /* Per-kernel-class CUDA-event timing on the dedisperser's compute stream (the analogue of pirate's
  * KernelTimer / ResourceTracker reporting, src_lib/GpuDedisperser.cpp:1674-1681). kernel_times()
- * synchronizes and returns accumulated milliseconds and launch counts for [grid, lds, stage1, stage2, pf]. */
+ * synchronizes and returns accumulated milliseconds and launch counts for [grid+lds (one fused kernel), unused, stage1, stage2, pf]. */
 int pb2_dd_enable_timing(pb2_dedisperser *dd, int on);
 int pb2_dd_kernel_times(pb2_dedisperser *dd, double *ms5, long *counts5);
 void pb2_dd_destroy(pb2_dedisperser *dd);

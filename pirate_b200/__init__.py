@@ -332,12 +332,12 @@ class GpuDedisperser:
         return n.value
 
     def algorithmic_bytes(self):
-        """HBM bytes per (chunk, batch) for [grid, lds, stage1, stage2, pf]."""
+        """HBM bytes per (chunk, batch) for [grid_lds, unused, stage1, stage2, pf]."""
         out = (ctypes.c_double * 5)()
         _check(lib().pb2_dd_algorithmic_bytes(self._h, out))
         return list(out)
 
-    KERNEL_CLASSES = ("grid", "lds", "stage1", "stage2", "pf")
+    KERNEL_CLASSES = ("grid_lds", "unused", "stage1", "stage2", "pf")
 
     def enable_timing(self, on=True):
         _check(lib().pb2_dd_enable_timing(self._h, 1 if on else 0))

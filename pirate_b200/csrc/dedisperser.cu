@@ -105,7 +105,7 @@ void GpuDedisperser::stop(std::exception_ptr e)
 
 int GpuDedisperser::kernels_per_batch() const
 {
-    return 1 + (plan.num_primary_trees > 1 ? 1 : 0) + int(plan.num_primary_trees) + 2 * int(plan.ntrees);
+    return 1 + int(plan.num_primary_trees) + 2 * int(plan.ntrees);
 }
 
 std::vector<double> GpuDedisperser::algorithmic_bytes() const
@@ -115,12 +115,10 @@ std::vector<double> GpuDedisperser::algorithmic_bytes() const
     // GpuLaggedDownsamplingKernel.cu:767-774, DedispersionKernel.cu:514-516, CoalescedDdKernel2.cu:128-135).
     double S = double(esize);
     long rank = plan.config.toplevel_tree_rank, nt = plan.nt_in;
+    // Fused gridding + lagged downsampling: read the input, write the level-0 tree and every level's rows.
     double grid = double(B) * (plan.nfreq + pow2(rank)) * nt * S;
     double lds = 0, st1 = 0, st2 = 0, pf = 0;
-    if (plan.num_primary_trees > 1) {
-        lds += double(B) * pow2(rank) * nt * S;
-        for (long p = 1; p < plan.num_primary_trees; p++) lds += double(B) * pow2(rank - 1) * (nt >> p) * S;
-    }
+    for (long p = 1; p < plan.num_primary_trees; p++) grid += double(B) * pow2(rank - 1) * (nt >> p) * S;
     for (long p = 0; p < plan.num_primary_trees; p++) {
         long rk = plan.stage1_dd_rank[p] + plan.stage1_amb_rank[p];
         st1 += 2.0 * B * pow2(rk) * (nt >> p) * S;
@@ -340,37 +338,28 @@ void GpuDedisperser::launch_batch(long seq_id)
     const int beam0 = int(ibatch * B);
     cudaStream_t s = compute;
 
-    GridArgs g;
+    GridLdsArgs g;
+    memset(&g, 0, sizeof(g));
     g.in = d_inputs.as<char>() + size_t(slot_in) * B * F * nt * esize;
-    g.out = d_tree0.ptr;
+    g.tree0 = d_tree0.ptr;
     g.chan_f0 = d_grid_f0.as<int>();
     g.chan_cnt = d_grid_cnt.as<int>();
     g.chan_woff = d_grid_woff.as<int>();
     g.chan_w = d_grid_w.as<float>();
-    g.F = int(F); g.N = int(N); g.T = int(nt);
+    g.F = int(F); g.rank = int(rank); g.T = int(nt); g.nlev = int(npri - 1);
+    for (long p = 1; p < npri; p++) {
+        g.ring[p - 1] = s1[p].lds.ptr;
+        g.cap_mask[p - 1] = s1[p].lds_cap - 1;
+    }
+    g.state = d_lds_state.as<float>();
+    g.lag_rank = (npri > 1) ? int(plan.stage1_dd_rank[1]) : 0;
+    g.ichunk = ichunk;
+    g.beam0 = beam0; g.B = int(B); g.total_beams = int(total_beams);
     cudaEvent_t t0 = tick(0, nullptr);
-    launch_grid(g, dtype_code, int(B), s);
+    launch_grid_lds(g, dtype_code, s);
     tick(0, t0);
     CUDA_CHECK(cudaEventRecord(ev_in_free[slot_in], s));
     in_free_recorded[slot_in] = true;
-
-    if (npri > 1) {
-        LdsArgs l;
-        memset(&l, 0, sizeof(l));
-        l.in = d_tree0.ptr;
-        l.rank = int(rank); l.T = int(nt); l.nlev = int(npri - 1);
-        for (long p = 1; p < npri; p++) {
-            l.ring[p - 1] = s1[p].lds.ptr;
-            l.cap_mask[p - 1] = s1[p].lds_cap - 1;
-        }
-        l.state = d_lds_state.as<float>();
-        l.lag_rank = int(plan.stage1_dd_rank[1]);
-        l.ichunk = ichunk;
-        l.beam0 = beam0; l.B = int(B); l.total_beams = int(total_beams);
-        cudaEvent_t t1 = tick(1, nullptr);
-        launch_lds(l, dtype_code, s);
-        tick(1, t1);
-    }
 
     for (long p = 0; p < npri; p++) {
         Stage1 &st = s1[p];

@@ -10,7 +10,7 @@
 //   tree0     (B, 2^rank, nt_in) level-0 tree                    storage dtype
 //   lds[p]    (total_beams, 2^(rank-1), cap_p) delay lines       storage dtype, cap_p = 2^k >= nt_p + 2^s1dd - 1
 //   ring[p]   per stage-1 output row (a, dm_brev): a delay line of capacity max_lag(row) + nt_p (rounded to 32)
-//   pfring[i] (total_beams, ndm_out, M, cap_i) subband rows       storage dtype, cap_i = 2^k >= nt + tpad + max subband lag
+//   pfring[i] (total_beams, ndm_out, M, cap_i) subband rows       storage dtype, cap_i = 2^k >= nt + tpad + Dout
 //   state     per-block tree state of the stage-1/stage-2 kernels (fp32): phase delay line + histories
 //   outputs   nbatches_out x per-tree (B, ndm_out, nt_out) out_max (storage dtype) + out_argmax (uint32)
 //   weights   nbatches_wt x per-tree (B, ndm_wt, nt_wt, P, N) fp32
@@ -81,11 +81,11 @@ public:
     // Number of kernels launched per (chunk, batch).
     int kernels_per_batch() const;
     // Bytes of HBM traffic per (chunk, batch) of each kernel class (algorithmic):
-    // [grid, lds, stage1, stage2, pf].
+    // [grid+lds (one fused kernel), unused, stage1, stage2, pf].
     std::vector<double> algorithmic_bytes() const;
 
     // Kernel timing: when enabled, CUDA events bracket each kernel class
-    // [grid, lds, stage1, stage2, pf] on the compute stream; kernel_times() synchronizes and returns
+    // [grid+lds (one fused kernel), unused, stage1, stage2, pf] on the compute stream; kernel_times() synchronizes and returns
     // the accumulated milliseconds and launch counts since the last reset.
     void enable_timing(bool on);
     void kernel_times(double *ms5, long *counts5);

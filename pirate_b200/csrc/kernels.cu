@@ -1,7 +1,8 @@
 // kernels.cu -- sm_100a kernels of the B200 dedispersion path.
 //
-//   grid_kernel    tree gridding                 (replaces GpuTreeGriddingKernel, src_lib/TreeGriddingKernel.cu:108-279)
-//   lds_kernel     lagged downsampling           (replaces GpuLaggedDownsamplingKernel, src_lib/GpuLaggedDownsamplingKernel.cu:668-918)
+//   grid_lds_kernel  tree gridding + lagged downsampling (replaces GpuTreeGriddingKernel,
+//                    src_lib/TreeGriddingKernel.cu:108-279, and GpuLaggedDownsamplingKernel,
+//                    src_lib/GpuLaggedDownsamplingKernel.cu:668-918)
 //   stage1_kernel  stage-1 tree -> delay lines   (replaces GpuDedispersionKernel outrb, src_lib/DedispersionKernel.cu:492-653)
 //   stage2_kernel  delay lines -> stage-2 tree
 //                  with subband outputs          (replaces the dd half of CoalescedDdKernel2, src_lib/CoalescedDdKernel2.cu:79-269)
@@ -47,132 +48,145 @@ static void check_launch(const char *what)
 
 
 // -------------------------------------------------------------------------------------------------
-// Tree gridding: out[b,n,t] = sum_f w[n,f] in[b,f,t], summed in ascending f from zero.
-// One warp per tree channel, 4 consecutive samples per lane.
-
-
-template<typename Ts>
-__global__ void __launch_bounds__(256) grid_kernel(GridArgs a)
-{
-    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int n = blockIdx.y * 8 + warp;
-    int t = (blockIdx.x * 32 + lane) * 4;
-    int b = blockIdx.z;
-    if (n >= a.N || t >= a.T)
-        return;
-
-    const Ts *in = (const Ts *) a.in + (long) b * a.F * a.T + t;
-    int f0 = a.chan_f0[n], cnt = a.chan_cnt[n], woff = a.chan_woff[n];
-    float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f, acc3 = 0.0f;
-
-    for (int k = 0; k < cnt; k++) {
-        float w = a.chan_w[woff + k];
-        const Ts *p = in + (long) (f0 + k) * a.T;
-        float x0, x1, x2, x3;
-        if constexpr (sizeof(Ts) == 4) {
-            float4 v = *(const float4 *) p;
-            x0 = v.x; x1 = v.y; x2 = v.z; x3 = v.w;
-        } else {
-            uint2 v = *(const uint2 *) p;
-            const Ts *h = (const Ts *) &v;
-            x0 = to_f(h[0]); x1 = to_f(h[1]); x2 = to_f(h[2]); x3 = to_f(h[3]);
-        }
-        acc0 = __fadd_rn(acc0, __fmul_rn(w, x0));
-        acc1 = __fadd_rn(acc1, __fmul_rn(w, x1));
-        acc2 = __fadd_rn(acc2, __fmul_rn(w, x2));
-        acc3 = __fadd_rn(acc3, __fmul_rn(w, x3));
-    }
-
-    Ts *out = (Ts *) a.out + ((long) b * a.N + n) * a.T + t;
-    if constexpr (sizeof(Ts) == 4) {
-        *(float4 *) out = make_float4(acc0, acc1, acc2, acc3);
-    } else {
-        uint2 v;
-        Ts *h = (Ts *) &v;
-        h[0] = from_f<Ts>(acc0); h[1] = from_f<Ts>(acc1); h[2] = from_f<Ts>(acc2); h[3] = from_f<Ts>(acc3);
-        *(uint2 *) out = v;
-    }
-}
-
-
-// -------------------------------------------------------------------------------------------------
-// Lagged downsampling. For each level p = 1..nlev:
+// Tree gridding fused with lagged downsampling.
+//
+// Gridding: tree channel n = sum_f w[n,f] in[f], summed in ascending f from zero with float(w)
+// overlap weights (ReferenceTreeGriddingKernel::apply, src_lib/TreeGriddingKernel.cu:62-102).
+// Lagged downsampling, for each level p = 1..nlev:
 //   ds_p[ch][u]  = (ds_{p-1}[ch][2u] + ds_{p-1}[ch][2u+1]) / sqrt2          (ds_0 = level-0 tree)
 //   out_p[c][u]  = (ds_p[2c][u-1] + ds_p[2c+1][u]) / sqrt2                     (one-sample lag on even channels)
 // out_p goes to a per-row delay line, written delayed by the per-row "large" lag
-// 2^s1dd - 1 - (c mod 2^s1dd) (ReferenceLaggedDownsamplingKernel.cpp:53-55), so that the stage-1
+// 2^s1dd - 1 - (c mod 2^s1dd) (ReferenceLaggedDownsamplingKernel.cpp:46-57), so that the stage-1
 // kernel reads aligned rows.
-// Each thread owns one output row c and a window of W0 level-0 samples.
+//
+// One thread per (beam, tree-channel pair (2c, 2c+1), window of W0 level-0 samples); consecutive
+// threads take consecutive windows, so every load and store is a contiguous run across the warp.
+// The thread grids both channels of its window (and writes them as the level-0 tree), builds every
+// level in registers, and gets the even channel's predecessor sample at each level by gridding the
+// 2^nlev samples before its window (at the chunk start: from a parity double-buffered state).
 
+
+// Loads W consecutive samples starting at p (16-byte vectors when W*sizeof(Ts) allows; p must then be
+// 16-byte aligned).
+template<typename Ts, int W>
+__device__ __forceinline__ void load_run(const Ts *p, float (&o)[W])
+{
+    if constexpr ((W * sizeof(Ts)) % 16 == 0) {
+        constexpr int PER = 16 / sizeof(Ts);
+#pragma unroll
+        for (int v = 0; v < W / PER; v++) {
+            uint4 q = ((const uint4 *) p)[v];
+            const Ts *h = (const Ts *) &q;
+#pragma unroll
+            for (int k = 0; k < PER; k++) o[v * PER + k] = to_f(h[k]);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < W; i++) o[i] = to_f(p[i]);
+    }
+}
+
+template<typename Ts, int W>
+__device__ __forceinline__ void store_run(Ts *p, const float (&o)[W])
+{
+    if constexpr ((W * sizeof(Ts)) % 16 == 0) {
+        constexpr int PER = 16 / sizeof(Ts);
+#pragma unroll
+        for (int v = 0; v < W / PER; v++) {
+            uint4 q;
+            Ts *h = (Ts *) &q;
+#pragma unroll
+            for (int k = 0; k < PER; k++) h[k] = from_f<Ts>(o[v * PER + k]);
+            ((uint4 *) p)[v] = q;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < W; i++) p[i] = from_f<Ts>(o[i]);
+    }
+}
+
+// Grids tree channel n over samples [t0, t0+W) of one beam's input (xb = beam base).
+template<typename Ts, int W>
+__device__ __forceinline__ void grid_run(const GridLdsArgs &a, const Ts *xb, long n, long t0, float (&o)[W])
+{
+#pragma unroll
+    for (int i = 0; i < W; i++) o[i] = 0.0f;
+    const int f0 = a.chan_f0[n], cnt = a.chan_cnt[n], woff = a.chan_woff[n];
+    for (int k = 0; k < cnt; k++) {
+        const float w = a.chan_w[woff + k];
+        float x[W];
+        load_run<Ts, W>(xb + (long) (f0 + k) * a.T + t0, x);
+#pragma unroll
+        for (int i = 0; i < W; i++) o[i] = __fadd_rn(o[i], __fmul_rn(w, x[i]));
+    }
+}
 
 template<typename Ts, int NLEV>
-__global__ void __launch_bounds__(128) lds_kernel(LdsArgs a)
+__global__ void __launch_bounds__(128) grid_lds_kernel(GridLdsArgs a)
 {
     constexpr int W0 = ((1 << NLEV) > 8) ? (1 << NLEV) : 8;
     constexpr int WE = 1 << NLEV;           // level-0 samples feeding one level-NLEV sample
 
-    long nhalf = 1L << (a.rank - 1);
-    long nwin = a.T / W0;
-    long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+    const long nhalf = 1L << (a.rank - 1);
+    const long nwin = a.T / W0;
+    const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nwin * nhalf * a.B)
         return;
-    int win = int(g % nwin);
-    long c = (g / nwin) % nhalf;
-    int b = int(g / (nwin * nhalf));
-    int bt = a.beam0 + b;
-    int parity = int(a.ichunk & 1);
+    const int win = int(g % nwin);
+    const long c = (g / nwin) % nhalf;
+    const int b = int(g / (nwin * nhalf));
+    const int bt = a.beam0 + b;
+    const int parity = int(a.ichunk & 1);
+    const long t0 = (long) win * W0;
 
-    const Ts *row0 = (const Ts *) a.in + ((long) b * (2 * nhalf) + 2 * c) * a.T;
-    const Ts *row1 = row0 + a.T;
-    long t0 = (long) win * W0;
+    const Ts *xb = (const Ts *) a.in + (long) b * a.F * a.T;
+    float r0[W0], r1[W0];
+    grid_run<Ts, W0>(a, xb, 2 * c, t0, r0);
+    grid_run<Ts, W0>(a, xb, 2 * c + 1, t0, r1);
+    Ts *lev0 = (Ts *) a.tree0 + ((long) b * (2 * nhalf) + 2 * c) * a.T + t0;
+    store_run<Ts, W0>(lev0, r0);
+    store_run<Ts, W0>(lev0 + a.T, r1);
 
-    float r0[W0], r1[W0], e[WE];
-#pragma unroll
-    for (int i = 0; i < W0; i++) {
-        r0[i] = to_f(row0[t0 + i]);
-        r1[i] = to_f(row1[t0 + i]);
-    }
-    if (win > 0) {
-#pragma unroll
-        for (int i = 0; i < WE; i++)
-            e[i] = to_f(row0[t0 - WE + i]);
-    }
+    if constexpr (NLEV > 0) {
+        float e[WE];
+        if (win > 0)
+            grid_run<Ts, WE>(a, xb, 2 * c, t0 - WE, e);
 
 #pragma unroll
-    for (int p = 1; p <= NLEV; p++) {
-        constexpr int dummy = 0; (void) dummy;
-        const int len = W0 >> p;
-        const int elen = WE >> p;
+        for (int p = 1; p <= NLEV; p++) {
+            const int len = W0 >> p;
+            const int elen = WE >> p;
 #pragma unroll
-        for (int u = 0; u < (W0 >> 1); u++) {
-            if (u < len) {
-                r0[u] = bfly(r0[2 * u], r0[2 * u + 1]);
-                r1[u] = bfly(r1[2 * u], r1[2 * u + 1]);
+            for (int u = 0; u < (W0 >> 1); u++) {
+                if (u < len) {
+                    r0[u] = bfly(r0[2 * u], r0[2 * u + 1]);
+                    r1[u] = bfly(r1[2 * u], r1[2 * u + 1]);
+                }
             }
-        }
-        float prev;
-        if (win > 0) {
+            float prev;
+            if (win > 0) {
 #pragma unroll
-            for (int u = 0; u < (WE >> 1); u++)
-                if (u < elen) e[u] = bfly(e[2 * u], e[2 * u + 1]);
-            prev = e[elen - 1];
-        } else {
-            prev = a.state[(((long) parity * a.total_beams + bt) * a.nlev + (p - 1)) * nhalf + c];
-        }
-
-        long cap = a.cap_mask[p - 1] + 1;
-        Ts *ring = (Ts *) a.ring[p - 1] + ((long) bt * nhalf + c) * cap;
-        long nt_p = a.T >> p;
-        long s_base = a.ichunk * nt_p + (long) win * len + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
-#pragma unroll
-        for (int u = 0; u < (W0 >> 1); u++) {
-            if (u < len) {
-                float lagged = (u == 0) ? prev : r0[u - 1];
-                ring[(s_base + u) & a.cap_mask[p - 1]] = from_f<Ts>(bfly(lagged, r1[u]));
+                for (int u = 0; u < (WE >> 1); u++)
+                    if (u < elen) e[u] = bfly(e[2 * u], e[2 * u + 1]);
+                prev = e[elen - 1];
+            } else {
+                prev = a.state[(((long) parity * a.total_beams + bt) * a.nlev + (p - 1)) * nhalf + c];
             }
+
+            const long cap = a.cap_mask[p - 1] + 1;
+            Ts *ring = (Ts *) a.ring[p - 1] + ((long) bt * nhalf + c) * cap;
+            const long nt_p = a.T >> p;
+            const long s_base = a.ichunk * nt_p + (long) win * len + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
+#pragma unroll
+            for (int u = 0; u < (W0 >> 1); u++) {
+                if (u < len) {
+                    float lagged = (u == 0) ? prev : r0[u - 1];
+                    ring[(s_base + u) & a.cap_mask[p - 1]] = from_f<Ts>(bfly(lagged, r1[u]));
+                }
+            }
+            if (win == nwin - 1)
+                a.state[(((long) (1 - parity) * a.total_beams + bt) * a.nlev + (p - 1)) * nhalf + c] = r0[len - 1];
         }
-        if (win == nwin - 1)
-            a.state[(((long) (1 - parity) * a.total_beams + bt) * a.nlev + (p - 1)) * nhalf + c] = r0[len - 1];
     }
 }
 
@@ -761,50 +775,37 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_fl
 // Host launchers.
 
 
-template<typename Ts>
-static void launch_grid_t(const GridArgs &a, int B, cudaStream_t s)
-{
-    dim3 grid((a.T / 4 + 31) / 32, (a.N + 7) / 8, B);
-    grid_kernel<Ts><<<grid, 256, 0, s>>>(a);
-    check_launch("grid_kernel");
-}
-
-void launch_grid(const GridArgs &a, int dtype, int B, cudaStream_t s)
-{
-    if (dtype == 0) launch_grid_t<float>(a, B, s);
-    else if (dtype == 1) launch_grid_t<__half>(a, B, s);
-    else launch_grid_t<__nv_bfloat16>(a, B, s);
-}
-
 template<typename Ts, int NLEV>
-static void launch_lds_t(const LdsArgs &a, cudaStream_t s)
+static void launch_grid_lds_t(const GridLdsArgs &a, cudaStream_t s)
 {
     constexpr int W0 = ((1 << NLEV) > 8) ? (1 << NLEV) : 8;
-    if (a.T % W0) throw std::runtime_error("lds_kernel: chunk length not a multiple of the window");
+    if (a.T % W0) throw std::runtime_error("grid_lds_kernel: chunk length not a multiple of the window");
     long nthr = (long) (a.T / W0) * (1L << (a.rank - 1)) * a.B;
-    lds_kernel<Ts, NLEV><<<(unsigned) ((nthr + 127) / 128), 128, 0, s>>>(a);
-    check_launch("lds_kernel");
+    grid_lds_kernel<Ts, NLEV><<<(unsigned) ((nthr + 127) / 128), 128, 0, s>>>(a);
+    check_launch("grid_lds_kernel");
 }
 
 template<typename Ts>
-static void launch_lds_d(const LdsArgs &a, cudaStream_t s)
+static void launch_grid_lds_d(const GridLdsArgs &a, cudaStream_t s)
 {
     switch (a.nlev) {
-    case 1: launch_lds_t<Ts, 1>(a, s); break;
-    case 2: launch_lds_t<Ts, 2>(a, s); break;
-    case 3: launch_lds_t<Ts, 3>(a, s); break;
-    case 4: launch_lds_t<Ts, 4>(a, s); break;
-    case 5: launch_lds_t<Ts, 5>(a, s); break;
-    case 6: launch_lds_t<Ts, 6>(a, s); break;
-    default: throw std::runtime_error("lds_kernel: unsupported number of levels");
+    case 0: launch_grid_lds_t<Ts, 0>(a, s); break;
+    case 1: launch_grid_lds_t<Ts, 1>(a, s); break;
+    case 2: launch_grid_lds_t<Ts, 2>(a, s); break;
+    case 3: launch_grid_lds_t<Ts, 3>(a, s); break;
+    case 4: launch_grid_lds_t<Ts, 4>(a, s); break;
+    case 5: launch_grid_lds_t<Ts, 5>(a, s); break;
+    case 6: launch_grid_lds_t<Ts, 6>(a, s); break;
+    default: throw std::runtime_error("grid_lds_kernel: unsupported number of levels");
     }
 }
 
-void launch_lds(const LdsArgs &a, int dtype, cudaStream_t s)
+void launch_grid_lds(const GridLdsArgs &a, int dtype, cudaStream_t s)
 {
-    if (dtype == 0) launch_lds_d<float>(a, s);
-    else if (dtype == 1) launch_lds_d<__half>(a, s);
-    else launch_lds_d<__nv_bfloat16>(a, s);
+    if (a.rank < 1) throw std::runtime_error("grid_lds_kernel: tree rank must be >= 1");
+    if (dtype == 0) launch_grid_lds_d<float>(a, s);
+    else if (dtype == 1) launch_grid_lds_d<__half>(a, s);
+    else launch_grid_lds_d<__nv_bfloat16>(a, s);
 }
 
 template<typename Ts, int RA, int RB>

@@ -93,23 +93,16 @@ struct PfArgs
     int beam0;
 };
 
-// Arguments of the tree-gridding kernel.
-struct GridArgs
+// Arguments of the fused tree-gridding + lagged-downsampling kernel.
+struct GridLdsArgs
 {
-    const void *in;         // (B, F, T) storage dtype
-    void *out;              // (B, N, T) storage dtype
-    const int *chan_f0;     // (N,) first input channel of tree channel n
-    const int *chan_cnt;    // (N,) number of input channels
-    const int *chan_woff;   // (N,) offset into chan_w
+    const void *in;         // input (B, F, T) storage dtype
+    void *tree0;            // level-0 tree (B, 2^rank, T) storage dtype
+    const int *chan_f0;     // (2^rank,) first input channel of tree channel n
+    const int *chan_cnt;    // (2^rank,) number of input channels
+    const int *chan_woff;   // (2^rank,) offset into chan_w
     const float *chan_w;    // overlap weights, ascending input channel
-    int F, N, T;
-};
-
-// Arguments of the lagged-downsampling kernel.
-struct LdsArgs
-{
-    const void *in;         // level-0 tree (B, 2^rank, T) storage dtype
-    int rank, T, nlev;      // nlev = num_primary_trees - 1
+    int F, rank, T, nlev;   // nlev = num_primary_trees - 1
     void *ring[6];          // per level p=1..nlev: delay lines (total_beams, 2^(rank-1), cap[p])
     long cap_mask[6];
     float *state;           // (2, total_beams, nlev, 2^(rank-1)) last even-channel sample per level
@@ -122,8 +115,7 @@ struct LdsArgs
 inline long stage1_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), false); }
 inline long stage2_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), true); }
 
-void launch_grid(const GridArgs &a, int dtype, int B, cudaStream_t s);
-void launch_lds(const LdsArgs &a, int dtype, cudaStream_t s);
+void launch_grid_lds(const GridLdsArgs &a, int dtype, cudaStream_t s);
 void launch_stage1(const Stage1Args &a, int dtype, int nblocks, int B, cudaStream_t s);
 void launch_stage2(const Stage2Args &a, int dtype, int nblocks, int B, cudaStream_t s);
 void launch_pf(const PfArgs &a, int dtype, int B, cudaStream_t s);

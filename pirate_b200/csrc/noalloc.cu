@@ -185,28 +185,21 @@ void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, cons
     auto T = [&](long o) { return base + tab_at + o; };
     auto P = [&](long o) { return base + o; };
 
-    GridArgs g;
+    GridLdsArgs g;
+    memset(&g, 0, sizeof(g));
     g.in = in;
-    g.out = P(tree0);
+    g.tree0 = P(tree0);
     g.chan_f0 = (const int *) T(t_f0);
     g.chan_cnt = (const int *) T(t_cnt);
     g.chan_woff = (const int *) T(t_woff);
     g.chan_w = (const float *) T(t_w);
-    g.F = int(F); g.N = int(N); g.T = int(nt);
-    launch_grid(g, dtype_code, int(B), stream);
-
-    if (npri > 1) {
-        LdsArgs l;
-        memset(&l, 0, sizeof(l));
-        l.in = P(tree0);
-        l.rank = int(rank); l.T = int(nt); l.nlev = int(npri - 1);
-        for (long p = 1; p < npri; p++) { l.ring[p - 1] = P(s1[p].lds); l.cap_mask[p - 1] = s1[p].lds_cap - 1; }
-        l.state = (float *) P(lds_state);
-        l.lag_rank = int(plan.stage1_dd_rank[1]);
-        l.ichunk = 0;
-        l.beam0 = 0; l.B = int(B); l.total_beams = int(B);
-        launch_lds(l, dtype_code, stream);
-    }
+    g.F = int(F); g.rank = int(rank); g.T = int(nt); g.nlev = int(npri - 1);
+    for (long p = 1; p < npri; p++) { g.ring[p - 1] = P(s1[p].lds); g.cap_mask[p - 1] = s1[p].lds_cap - 1; }
+    g.state = (float *) P(lds_state);
+    g.lag_rank = (npri > 1) ? int(plan.stage1_dd_rank[1]) : 0;
+    g.ichunk = 0;
+    g.beam0 = 0; g.B = int(B); g.total_beams = int(B);
+    launch_grid_lds(g, dtype_code, stream);
 
     for (long p = 0; p < npri; p++) {
         S1 &st = s1[p];
