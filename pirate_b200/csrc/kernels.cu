@@ -772,6 +772,285 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_fl
 
 
 // -------------------------------------------------------------------------------------------------
+// Fast peak finding (output time downsampling Dout >= 4; the general kernel above covers the rest).
+//
+// Same work split (one warp per beam, coarse dm and 32 output times; lane = output time) and the same
+// results, organised around three changes:
+//
+//  1. Bank-conflict-free shared memory. Level l of the boxcar window is stored in blocks of nsamp_l
+//     entries (one block per lane: its output time's fine samples), each followed by a pad of 2
+//     floats (1 for levels read one float at a time). A lane's block is contiguous and the 32 blocks
+//     fall on distinct banks for 8-byte (or 4-byte) accesses.
+//  2. Levels are built while they are scanned: while a lane scans its fine samples at level l two at
+//     a time, the pair's sum is its level-(l+1) entry (B_{l+1}[u] = B_l[2u] + B_l[2u+1] while
+//     dt doubles), so only the pad region before the first output time and the levels with
+//     saturated time step (dt = Dcore) are built in a separate pass.
+//  3. Max-only trial loop. The scan keeps, per group (level, multiplet), only the maximum trial value
+//     (fmaxf, which ignores NaN as the reference's strict '>' does), and across groups the first
+//     group, in the reference's (level, multiplet) order, whose maximum equals the overall one. At the
+//     end each lane recomputes the trials of its winning group from the delay line (every boxcar is a
+//     pairwise tree sum of consecutive samples, the reference's rounding) and takes the first trial,
+//     in (fine time, profile) order, equal to the maximum: its value and token are the outputs.
+
+// Per-level constants of the fast peak finder (host-computed; level l has time step dt, boxcar
+// length 2^l = S*dt, and nsamp = Dout/dt fine samples per output time).
+enum { kPfU = 1, kPfPairs = 2, kPfNextU = 4 };
+struct PfGeom
+{
+    int off[kPfMaxLevels];   // first float of level l in a warp's region (even)
+    int e[kPfMaxLevels];     // entry i lies in block (i + e) >> k
+    int k[kPfMaxLevels];     // log2(nsamp_l)
+    int pad[kPfMaxLevels];   // floats after each block
+    int I[kPfMaxLevels];     // entry of the warp's first output time's first fine sample
+    int n[kPfMaxLevels];     // entries of level l in the window of 32 output times
+    int dt[kPfMaxLevels], S[kPfMaxLevels], nsamp[kPfMaxLevels];
+    int rr[kPfMaxLevels], ss[kPfMaxLevels];   // B_l[u] = B_{l-1}[rr u] + B_{l-1}[rr u + ss]
+    int flags[kPfMaxLevels]; // kPfU: dt = 2^l; kPfPairs: scanned two fine samples at a time;
+                             // kPfNextU: level l+1 has dt = 2^(l+1) and is built by this level's scan
+    int warp_floats;
+};
+
+// max(a, b, c) ignoring NaN inputs (sm_100 three-input max).
+__device__ __forceinline__ float pf_max3(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+__device__ __forceinline__ int pf_phys(const PfGeom &g, int l, int i)
+{
+    const int t = i + g.e[l];
+    return g.off[l] + t + g.pad[l] * (t >> g.k[l]);
+}
+
+template<typename Ts> __device__ __forceinline__ void pf_load4(const Ts *p, float (&v)[4]);
+template<> __device__ __forceinline__ void pf_load4<float>(const float *p, float (&v)[4])
+{
+    const float4 q = *(const float4 *) p;
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+template<> __device__ __forceinline__ void pf_load4<__half>(const __half *p, float (&v)[4])
+{
+    const uint2 q = *(const uint2 *) p;
+    const float2 a = __half22float2(*(const __half2 *) &q.x), b = __half22float2(*(const __half2 *) &q.y);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+template<> __device__ __forceinline__ void pf_load4<__nv_bfloat16>(const __nv_bfloat16 *p, float (&v)[4])
+{
+    const uint2 q = *(const uint2 *) p;
+    const float2 a = __bfloat1622float2(*(const __nv_bfloat162 *) &q.x), b = __bfloat1622float2(*(const __nv_bfloat162 *) &q.y);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+// Boxcar of 2^l samples starting at window sample t, as a pairwise tree sum (the reference's level
+// recursion B_{l+1}(t) = B_l(t) + B_l(t + 2^l) unrolled down to the samples). l <= 4.
+template<typename Ts>
+__device__ __forceinline__ float pf_tsum(const Ts *row, int sbm, int mask, int t, int l)
+{
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+        v[i] = (i < (1 << l)) ? to_f(row[(sbm + t + i) & mask]) : 0.0f;
+#pragma unroll
+    for (int st = 0; st < 4; st++) {
+        if (st < l) {
+#pragma unroll
+            for (int i = 0; i < (8 >> st); i++)
+                v[i] = __fadd_rn(v[2 * i], v[2 * i + 1]);
+        }
+    }
+    return v[0];
+}
+
+template<typename Ts, int L>
+__global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom g)
+{
+    extern __shared__ float sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int dm = blockIdx.y * kPfWarps + warp;
+    const int b = blockIdx.z, bt = a.beam0 + b;
+    const int tout0 = blockIdx.x * 32;
+    if (dm >= a.ndm_out)
+        return;   // whole warp exits; warps never synchronize across the block
+
+    const int ntw = min(32, a.nt_out - tout0);
+    const int tout = tout0 + lane;
+    const bool active = (lane < ntw);
+    float *lev = sm + warp * g.warp_floats;
+
+    const int Dout = a.Dout;
+    const int Wds = a.ndm_out / a.ndm_wt, Tds = a.nt_out / a.nt_wt;
+    const float *wp = a.wt + ((((long) b * a.ndm_wt + dm / Wds) * a.nt_wt + (active ? tout / Tds : 0)) * a.P) * a.N;
+    const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
+    const int mask = int(a.pf_cap - 1);
+    // Window sample 0 (stream time s0 + 32 tile * Dout - tpad, a multiple of 4), as a delay-line slot.
+    const int sbm = int((a.s0 + (long) tout0 * Dout - a.tpad) & (a.pf_cap - 1));
+    const bool full = (L > 1) || (a.P > 1);
+    const int nq0 = (ntw * Dout + a.tpad) >> 2;   // samples the active lanes read (a partial last tile reads fewer)
+
+    float best = -1.0e30f;
+    int winG = -1;            // group l * M + m of the first maximum; -1: no trial above -1e30
+    int winP = 0;             // first fine sample (pair) of that group holding the maximum
+
+    for (int m = 0; m < a.M; m++) {
+        const Ts *row = pfrows + (long) m * a.pf_cap;
+
+        // Level 0: the window's samples, four per lane and step (4-aligned runs never wrap the line).
+        for (int q = lane; q < nq0; q += 32) {
+            float v[4];
+            pf_load4<Ts>(row + ((sbm + 4 * q) & mask), v);
+            float *d = lev + pf_phys(g, 0, 4 * q);
+            *(float2 *) d = make_float2(v[0], v[1]);
+            *(float2 *) (d + 2) = make_float2(v[2], v[3]);
+        }
+        __syncwarp();
+
+        const int n = a.m_to_n[m];
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const int S = g.S[l], nsamp = g.nsamp[l];
+            const bool U = g.flags[l] & kPfU;
+            const bool nextU = (l + 1 < L) && (g.flags[l] & kPfNextU);
+
+            if (l > 0 && !U) {
+                // Saturated level (dt = Dcore): B_l[u] = B_{l-1}[rr u] + B_{l-1}[rr u + ss].
+                const int rr = g.rr[l], ss = g.ss[l];
+                for (int u = lane; u < g.n[l]; u += 32)
+                    lev[pf_phys(g, l, u)] = __fadd_rn(lev[pf_phys(g, l - 1, rr * u)], lev[pf_phys(g, l - 1, rr * u + ss)]);
+                __syncwarp();
+            }
+            if (nextU) {
+                // Entries of level l+1 before the first output time.
+                for (int u = lane; u < g.I[l + 1]; u += 32)
+                    lev[pf_phys(g, l + 1, u)] = __fadd_rn(lev[pf_phys(g, l, 2 * u)], lev[pf_phys(g, l, 2 * u + 1)]);
+            }
+
+            float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f;
+            if (l == 0) w0 = wp[n];
+            if (full) {
+                w1 = wp[(3 * l + 1) * a.N + n];
+                w2 = wp[(3 * l + 2) * a.N + n];
+                w3 = wp[(3 * l + 3) * a.N + n];
+            }
+
+            const int j0 = g.I[l] + lane * nsamp;
+            float gmax = -1.0e30f;
+            int gp = 0;   // first fine sample (pair start) whose trials reach gmax
+            if (g.flags[l] & kPfPairs) {
+                // x0..x3 = x[is-3..is]; carried: x2, hx1 = x[is-2]/2, hx2 = x[is-1]/2, Ap = x[is-3]/2 + x[is-2].
+                float x2 = lev[pf_phys(g, l, j0 - 1)];
+                const float x1 = lev[pf_phys(g, l, j0 - 2)];
+                const float x0 = lev[pf_phys(g, l, j0 - 3)];
+                float hx1 = __fmul_rn(0.5f, x1), hx2 = __fmul_rn(0.5f, x2);
+                float Ap = __fadd_rn(__fmul_rn(0.5f, x0), x1);
+                const float *xs = lev + pf_phys(g, l, j0);
+                float *ys = lev + (nextU ? pf_phys(g, l + 1, g.I[l + 1] + lane * (nsamp >> 1)) : 0);
+
+#pragma unroll 2
+                for (int is = 0; is < nsamp; is += 2) {
+                    const float2 xx = *(const float2 *) (xs + is);
+                    const float xa = xx.x, xb = xx.y;
+                    float mx;
+                    if (full) {
+                        // fine sample is (xa) and is+1 (xb): profiles y1 = x2+x3, y2 = (x1/2+x2)+x3/2,
+                        // y3 = ((x0/2+x1)+x2)+x3/2 with the reference's association.
+                        const float ha = __fmul_rn(0.5f, xa), hb = __fmul_rn(0.5f, xb);
+                        const float Aa = __fadd_rn(hx1, x2), Ab = __fadd_rn(hx2, xa);
+                        const float v1a = __fmul_rn(w1, __fadd_rn(x2, xa));
+                        const float v2a = __fmul_rn(w2, __fadd_rn(Aa, ha));
+                        const float v3a = __fmul_rn(w3, __fadd_rn(__fadd_rn(Ap, x2), ha));
+                        const float v1b = __fmul_rn(w1, __fadd_rn(xa, xb));
+                        const float v2b = __fmul_rn(w2, __fadd_rn(Ab, hb));
+                        const float v3b = __fmul_rn(w3, __fadd_rn(__fadd_rn(Aa, xa), hb));
+                        if (l == 0) {
+                            const float t = pf_max3(__fmul_rn(w0, xa), v1a, v2a);
+                            mx = fmaxf(pf_max3(t, v3a, __fmul_rn(w0, xb)), pf_max3(v1b, v2b, v3b));
+                        } else {
+                            mx = fmaxf(pf_max3(v1a, v2a, v3a), pf_max3(v1b, v2b, v3b));
+                        }
+                        hx1 = ha; hx2 = hb; x2 = xb; Ap = Ab;
+                    } else {
+                        mx = fmaxf(__fmul_rn(w0, xa), __fmul_rn(w0, xb));
+                    }
+                    if (mx > gmax) { gmax = mx; gp = is; }
+                    if (nextU) ys[is >> 1] = __fadd_rn(xa, xb);
+                }
+            } else {
+                for (int is = 0; is < nsamp; is++) {
+                    const int j = j0 + is;
+                    const float x3 = lev[pf_phys(g, l, j)];
+                    float v = (l == 0) ? __fmul_rn(w0, x3) : -1.0e30f;
+                    if (full) {
+                        const float x0 = lev[pf_phys(g, l, j - 3 * S)];
+                        const float x1 = lev[pf_phys(g, l, j - 2 * S)];
+                        const float x2 = lev[pf_phys(g, l, j - S)];
+                        const float hx3 = __fmul_rn(0.5f, x3);
+                        const float y1 = __fadd_rn(x2, x3);
+                        const float y2 = __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3);
+                        const float y3 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3);
+                        v = fmaxf(v, pf_max3(__fmul_rn(w1, y1), __fmul_rn(w2, y2), __fmul_rn(w3, y3)));
+                    }
+                    if (v > gmax) { gmax = v; gp = is; }
+                }
+            }
+            __syncwarp();
+
+            const int G = l * a.M + m;
+            if (gmax > best || (gmax == best && G < winG)) {
+                best = gmax;
+                winG = G;
+                winP = gp;
+            }
+        }
+    }
+
+    if (!active)
+        return;
+
+    // Recompute the trials of the winning group's first maximal fine sample (or pair) in the
+    // reference's order; the first equal to the maximum wins.
+    float outv = best;
+    uint32_t tok = 0xffffffffu;
+    if (winG >= 0) {
+        const int l = winG / a.M, m = winG - l * a.M;
+        const int dt = g.dt[l], S = g.S[l], nsamp = g.nsamp[l];
+        const int n = a.m_to_n[m];
+        const float w0 = (l == 0) ? wp[n] : 0.0f;
+        const float w1 = full ? wp[(3 * l + 1) * a.N + n] : 0.0f;
+        const float w2 = full ? wp[(3 * l + 2) * a.N + n] : 0.0f;
+        const float w3 = full ? wp[(3 * l + 3) * a.N + n] : 0.0f;
+        const Ts *row = pfrows + (long) m * a.pf_cap;
+        const int j0 = g.I[l] + lane * nsamp;
+        for (int is = winP; is < min(winP + 2, nsamp); is++) {
+            const int j = j0 + is;
+            const float x3 = pf_tsum<Ts>(row, sbm, mask, j * dt, l);
+            const uint32_t tk0 = (uint32_t(m) << 16) | uint32_t(is * dt);
+            if (l == 0) {
+                const float v0 = __fmul_rn(w0, x3);
+                if (v0 == best) { outv = v0; tok = tk0; break; }
+            }
+            if (full) {
+                const float x0 = pf_tsum<Ts>(row, sbm, mask, (j - 3 * S) * dt, l);
+                const float x1 = pf_tsum<Ts>(row, sbm, mask, (j - 2 * S) * dt, l);
+                const float x2 = pf_tsum<Ts>(row, sbm, mask, (j - S) * dt, l);
+                const float hx3 = __fmul_rn(0.5f, x3);
+                const float v1 = __fmul_rn(w1, __fadd_rn(x2, x3));
+                const float v2 = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3));
+                const float v3 = __fmul_rn(w3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3));
+                if (v1 == best) { outv = v1; tok = tk0 | (uint32_t(3 * l + 1) << 8); break; }
+                if (v2 == best) { outv = v2; tok = tk0 | (uint32_t(3 * l + 2) << 8); break; }
+                if (v3 == best) { outv = v3; tok = tk0 | (uint32_t(3 * l + 3) << 8); break; }
+            }
+        }
+    }
+    const long o = ((long) b * a.ndm_out + dm) * a.nt_out + tout;
+    ((Ts *) a.out_max)[o] = from_f<Ts>(outv);
+    a.out_argmax[o] = tok;
+}
+
+
+// -------------------------------------------------------------------------------------------------
 // Host launchers.
 
 
@@ -882,9 +1161,60 @@ int pf_warp_floats(int Dout, int tpad, int Dcore, int L)
     return tot;
 }
 
+// Shared-memory layout of the fast peak finder for one warp (see PfGeom).
+static PfGeom pf_geom(int Dout, int Dcore, int tpad, int L)
+{
+    PfGeom g{};
+    int off = 0;
+    for (int l = 0; l < L; l++) {
+        const int dt = (Dcore < (1 << l)) ? Dcore : (1 << l);
+        const int nsamp = Dout / dt;
+        const bool pairs = ((1 << l) <= Dcore) && nsamp >= 2;
+        const int I = (tpad + dt - (1 << l)) / dt;
+        int k = 0;
+        while ((1 << k) < nsamp) k++;
+        g.off[l] = off;
+        g.e[l] = (nsamp - I % nsamp) % nsamp;
+        g.k[l] = k;
+        g.pad[l] = pairs ? (nsamp >= 4 ? 2 : 0) : (nsamp >= 2 ? 1 : 0);
+        g.I[l] = I;
+        g.n[l] = 32 * nsamp + I;
+        g.dt[l] = dt;
+        g.S[l] = (1 << l) / dt;
+        g.nsamp[l] = nsamp;
+        if (l > 0) {
+            const int dtp = (Dcore < (1 << (l - 1))) ? Dcore : (1 << (l - 1));
+            g.rr[l] = dt / dtp;
+            g.ss[l] = (1 << (l - 1)) / dtp;
+        }
+        g.flags[l] = (((1 << l) <= Dcore) ? kPfU : 0) | (pairs ? kPfPairs : 0)
+                   | ((l + 1 < L && (2 << l) <= Dcore) ? kPfNextU : 0);
+        const int t = g.n[l] - 1 + g.e[l];
+        const int size = t + g.pad[l] * (t >> k) + 1;
+        off += (size + 1) & ~1;
+    }
+    g.warp_floats = off;
+    return g;
+}
+
+// The fast kernel needs 4-sample runs of the window (Dout >= 4, tpad and s0 multiples of 4).
+static bool pf_fast_ok(const PfArgs &a)
+{
+    return a.Dout >= 4 && (a.tpad % 4) == 0 && (a.s0 % 4) == 0 && (a.pf_cap % 4) == 0 && a.L <= 5;
+}
+
 template<typename Ts, int L>
 static void launch_pf_l(const PfArgs &a, int B, cudaStream_t s)
 {
+    if (pf_fast_ok(a)) {
+        const PfGeom g = pf_geom(a.Dout, a.Dcore, a.tpad, L);
+        size_t sm = (size_t) kPfWarps * g.warp_floats * sizeof(float);
+        set_smem(pf_fast_kernel<Ts, L>, sm);
+        dim3 grid((a.nt_out + 31) / 32, (a.ndm_out + kPfWarps - 1) / kPfWarps, B);
+        pf_fast_kernel<Ts, L><<<grid, kPfWarps * 32, sm, s>>>(a, g);
+        check_launch("pf_fast_kernel");
+        return;
+    }
     int wf = pf_warp_floats(a.Dout, a.tpad, a.Dcore, a.L);
     size_t sm = (size_t) kPfWarps * wf * sizeof(float);
     set_smem(pf_kernel<Ts, L>, sm);

@@ -22,15 +22,21 @@ FP32_CASES = [
     (10, 1024, 512, [0, 0, 1], [(0, 32), (0, 16), (0, 8)], 1, 1),
     (11, 2000, 256, [3, 5, 3, 1], [(2, 8), (1, 4)], 4, 2),
     (7, 50, 128, [1, 1], [(0, 1), (0, 2)], 3, 1),
+    # explicit output time downsampling (third entry): 16 and 32 (saturated boxcar levels, partial
+    # 32-output tiles), 64, 2 and 1
+    (8, 256, 512, [0, 1, 1], [(0, 32, 16), (0, 16, 32)], 2, 1),
+    (7, 128, 512, [1, 1], [(0, 8, 64), (0, 4, 2), (0, 2, 1)], 1, 1),
 ]
 
 
 def _cfg(case, dtype="float32"):
     rank, nfreq, nt, sb, pts, bpg, bpb = case
     prim = []
-    for ip, (net, w) in enumerate(pts):
-        prim.append(dict(num_early_triggers=net, max_width=w, dm_downsampling=0, time_downsampling=0,
-                         wt_dm_downsampling=2 ** ((rank - (1 if ip else 0) - net) // 2), wt_time_downsampling=16))
+    for ip, pt in enumerate(pts):
+        net, w = pt[:2]
+        tds = pt[2] if len(pt) > 2 else 0
+        prim.append(dict(num_early_triggers=net, max_width=w, dm_downsampling=0, time_downsampling=tds,
+                         wt_dm_downsampling=2 ** ((rank - (1 if ip else 0) - net) // 2), wt_time_downsampling=max(16, tds)))
     return H.toy_config(rank=rank, nfreq=nfreq, nt=nt, dtype=dtype, subbands=sb, beams_per_gpu=bpg,
                         beams_per_batch=bpb, num_active_batches=1, primary_trees=prim)
 
@@ -55,6 +61,35 @@ def test_fp32_bitwise(pb2lib, case):
                 pytest.fail("seq %d tree %d: out_max differs at %d/%d entries, max |diff| %.3g" % (seq, i, (d > 0).sum(), d.size, d.max()))
             if not np.array_equal(ga, oa):
                 pytest.fail("seq %d tree %d: out_argmax differs at %d/%d entries" % (seq, i, (ga != oa).sum(), ga.size))
+
+
+@pytest.mark.parametrize("case", [FP32_CASES[1], FP32_CASES[6]], ids=["r8_tds4", "r8_tds16_32"])
+def test_fp32_nan_inputs(pb2lib, case):
+    """Inputs with NaN samples: NaN propagates through the trees; the peak finder ignores NaN trials
+    (the reference's strict '>' never takes one) and reports -1e30 / token 0xffffffff where every trial
+    is NaN. float32 outputs and tokens must still match the oracle exactly."""
+    cfg = _cfg(case)
+    nb = cfg["beams_per_gpu"] // cfg["beams_per_batch"]
+    nchunks = 3
+    xs = H.make_inputs(cfg, nchunks, seed=5)
+    rng = np.random.default_rng(17)
+    for x in xs:
+        x[rng.random(x.shape) < 2e-4] = np.nan
+    xs[nb][:, :, 100:104] = np.nan   # a NaN burst in every channel: some outputs see only NaN trials
+    orc, _ = H.run_oracle(cfg, xs[:0], [])
+    ws = H.make_weights(orc, seed=2, nbatches_wt=1)
+    _, ores = H.run_oracle(cfg, xs, ws, 1, 32)
+    plan, dd, gres = H.run_gpu(pb2lib, cfg, xs, ws)
+    nan_trials = 0
+    for seq in range(nchunks * nb):
+        for i in range(orc.ntrees):
+            gm, ga = gres[seq][0][i], gres[seq][1][i]
+            om, oa = ores[seq][0][i], ores[seq][1][i]
+            nan_trials += int((oa == 0xffffffff).sum())
+            assert np.array_equal(gm, om, equal_nan=True), "seq %d tree %d: out_max differs" % (seq, i)
+            assert np.array_equal(ga, oa), "seq %d tree %d: out_argmax differs at %d entries" % (seq, i, (ga != oa).sum())
+    assert not np.isnan(np.concatenate([r.ravel() for s in ores for r in s[0]])).any()
+    assert nan_trials > 0   # the burst left outputs without a winning trial
 
 
 LOWP_CASES = [
