@@ -401,6 +401,12 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
     unsigned s = (unsigned) __cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" :: "r"(s), "l"(gmem) : "memory");
 }
+template<int BYTES>
+__device__ __forceinline__ void cp_async_bytes(void *smem, const void *gmem)
+{
+    unsigned s = (unsigned) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" :: "r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
@@ -775,22 +781,25 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_fl
 // Fast peak finding (output time downsampling Dout >= 4; the general kernel above covers the rest).
 //
 // Same work split (one warp per beam, coarse dm and 32 output times; lane = output time) and the same
-// results, organised around three changes:
+// results, organised around four changes:
 //
 //  1. Bank-conflict-free shared memory. Level l of the boxcar window is stored in blocks of nsamp_l
-//     entries (one block per lane: its output time's fine samples), each followed by a pad of 2
-//     floats (1 for levels read one float at a time). A lane's block is contiguous and the 32 blocks
-//     fall on distinct banks for 8-byte (or 4-byte) accesses.
+//     entries (one block per lane: its output time's fine samples). Levels scanned in pairs with
+//     blocks of >= 4 entries pad each block with 2 floats, so the 32 blocks fall on distinct banks
+//     for 8-byte loads; the other levels are contiguous and are read in pairs or single floats.
 //  2. Levels are built while they are scanned: while a lane scans its fine samples at level l two at
 //     a time, the pair's sum is its level-(l+1) entry (B_{l+1}[u] = B_l[2u] + B_l[2u+1] while
 //     dt doubles), so only the pad region before the first output time and the levels with
 //     saturated time step (dt = Dcore) are built in a separate pass.
-//  3. Max-only trial loop. The scan keeps, per group (level, multiplet), only the maximum trial value
-//     (fmaxf, which ignores NaN as the reference's strict '>' does), and across groups the first
-//     group, in the reference's (level, multiplet) order, whose maximum equals the overall one. At the
-//     end each lane recomputes the trials of its winning group from the delay line (every boxcar is a
-//     pairwise tree sum of consecutive samples, the reference's rounding) and takes the first trial,
-//     in (fine time, profile) order, equal to the maximum: its value and token are the outputs.
+//  3. Max-only trial loop. The scan keeps, per group (level, multiplet), the maximum trial value
+//     (fmaxf and the three-input max, which ignore NaN as the reference's strict '>' does) and the
+//     first fine sample (pair) reaching it; across groups, the first group in the reference's
+//     (level, multiplet) order whose maximum equals the overall one. After each multiplet, a lane
+//     whose maximum moved into it recomputes that fine sample's (pair's) trials from shared memory
+//     and takes the first, in (fine time, profile) order, equal to the maximum: its value and token
+//     are the outputs.
+//  4. The next multiplet's window is staged in shared memory with cp.async while the current one is
+//     scanned.
 
 // Per-level constants of the fast peak finder (host-computed; level l has time step dt, boxcar
 // length 2^l = S*dt, and nsamp = Dout/dt fine samples per output time).
@@ -807,6 +816,7 @@ struct PfGeom
     int rr[kPfMaxLevels], ss[kPfMaxLevels];   // B_l[u] = B_{l-1}[rr u] + B_{l-1}[rr u + ss]
     int flags[kPfMaxLevels]; // kPfU: dt = 2^l; kPfPairs: scanned two fine samples at a time;
                              // kPfNextU: level l+1 has dt = 2^(l+1) and is built by this level's scan
+    int raw_off;             // staging buffer of the window's raw samples (16-byte aligned)
     int warp_floats;
 };
 
@@ -843,26 +853,6 @@ template<> __device__ __forceinline__ void pf_load4<__nv_bfloat16>(const __nv_bf
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
-// Boxcar of 2^l samples starting at window sample t, as a pairwise tree sum (the reference's level
-// recursion B_{l+1}(t) = B_l(t) + B_l(t + 2^l) unrolled down to the samples). l <= 4.
-template<typename Ts>
-__device__ __forceinline__ float pf_tsum(const Ts *row, int sbm, int mask, int t, int l)
-{
-    float v[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++)
-        v[i] = (i < (1 << l)) ? to_f(row[(sbm + t + i) & mask]) : 0.0f;
-#pragma unroll
-    for (int st = 0; st < 4; st++) {
-        if (st < l) {
-#pragma unroll
-            for (int i = 0; i < (8 >> st); i++)
-                v[i] = __fadd_rn(v[2 * i], v[2 * i + 1]);
-        }
-    }
-    return v[0];
-}
-
 template<typename Ts, int L>
 __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom g)
 {
@@ -891,22 +881,38 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom
 
     float best = -1.0e30f;
     int winG = -1;            // group l * M + m of the first maximum; -1: no trial above -1e30
-    int winP = 0;             // first fine sample (pair) of that group holding the maximum
+    float outv = best;        // value and token of the first maximal trial
+    uint32_t tok = 0xffffffffu;
+
+    // The window's raw samples are staged with cp.async one multiplet ahead (4-sample runs: a
+    // 4-aligned run never wraps the delay line).
+    Ts *raw = (Ts *) (lev + g.raw_off);
+    auto stage = [&](int m) {
+        const Ts *row = pfrows + (long) m * a.pf_cap;
+        for (int q = lane; q < nq0; q += 32)
+            cp_async_bytes<4 * sizeof(Ts)>(raw + 4 * q, row + ((sbm + 4 * q) & mask));
+        cp_async_commit();
+    };
+    stage(0);
 
     for (int m = 0; m < a.M; m++) {
-        const Ts *row = pfrows + (long) m * a.pf_cap;
-
-        // Level 0: the window's samples, four per lane and step (4-aligned runs never wrap the line).
+        // Level 0: the window's samples from the staging buffer; then stage the next multiplet.
+        cp_async_wait0();
+        __syncwarp();
         for (int q = lane; q < nq0; q += 32) {
             float v[4];
-            pf_load4<Ts>(row + ((sbm + 4 * q) & mask), v);
+            pf_load4<Ts>(raw + 4 * q, v);
             float *d = lev + pf_phys(g, 0, 4 * q);
             *(float2 *) d = make_float2(v[0], v[1]);
             *(float2 *) (d + 2) = make_float2(v[2], v[3]);
         }
         __syncwarp();
+        if (m + 1 < a.M)
+            stage(m + 1);
 
         const int n = a.m_to_n[m];
+        bool upd = false;     // this lane's maximum moved to a group of this multiplet
+        int winL = 0, winP = 0;
 #pragma unroll
         for (int l = 0; l < L; l++) {
             const int S = g.S[l], nsamp = g.nsamp[l];
@@ -977,21 +983,41 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom
                     if (nextU) ys[is >> 1] = __fadd_rn(xa, xb);
                 }
             } else {
-                for (int is = 0; is < nsamp; is++) {
-                    const int j = j0 + is;
-                    const float x3 = lev[pf_phys(g, l, j)];
+                // Levels stored without padding (contiguous across lanes): x[j - k S] = xb[is - k S].
+                const float *xb = lev + pf_phys(g, l, j0);
+                if (nsamp >= 2) {
+                    // Two fine samples at a time (S and nsamp even: 8-byte aligned pairs).
+                    for (int is = 0; is < nsamp; is += 2) {
+                        const float2 p3 = *(const float2 *) (xb + is), p2 = *(const float2 *) (xb + is - S);
+                        const float2 p1 = *(const float2 *) (xb + is - 2 * S), p0 = *(const float2 *) (xb + is - 3 * S);
+                        float mx;
+                        if (full) {
+                            const float ha = __fmul_rn(0.5f, p3.x), hb = __fmul_rn(0.5f, p3.y);
+                            const float v1a = __fmul_rn(w1, __fadd_rn(p2.x, p3.x));
+                            const float v2a = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, p1.x), p2.x), ha));
+                            const float v3a = __fmul_rn(w3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, p0.x), p1.x), p2.x), ha));
+                            const float v1b = __fmul_rn(w1, __fadd_rn(p2.y, p3.y));
+                            const float v2b = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, p1.y), p2.y), hb));
+                            const float v3b = __fmul_rn(w3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, p0.y), p1.y), p2.y), hb));
+                            mx = fmaxf(pf_max3(v1a, v2a, v3a), pf_max3(v1b, v2b, v3b));
+                            if (l == 0) mx = pf_max3(mx, __fmul_rn(w0, p3.x), __fmul_rn(w0, p3.y));
+                        } else {
+                            mx = fmaxf(__fmul_rn(w0, p3.x), __fmul_rn(w0, p3.y));
+                        }
+                        if (mx > gmax) { gmax = mx; gp = is; }
+                    }
+                } else {
+                    const float x3 = xb[0];
                     float v = (l == 0) ? __fmul_rn(w0, x3) : -1.0e30f;
                     if (full) {
-                        const float x0 = lev[pf_phys(g, l, j - 3 * S)];
-                        const float x1 = lev[pf_phys(g, l, j - 2 * S)];
-                        const float x2 = lev[pf_phys(g, l, j - S)];
+                        const float x0 = xb[-3 * S], x1 = xb[-2 * S], x2 = xb[-S];
                         const float hx3 = __fmul_rn(0.5f, x3);
                         const float y1 = __fadd_rn(x2, x3);
                         const float y2 = __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3);
                         const float y3 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3);
                         v = fmaxf(v, pf_max3(__fmul_rn(w1, y1), __fmul_rn(w2, y2), __fmul_rn(w3, y3)));
                     }
-                    if (v > gmax) { gmax = v; gp = is; }
+                    if (v > gmax) { gmax = v; gp = 0; }
                 }
             }
             __syncwarp();
@@ -1000,50 +1026,53 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom
             if (gmax > best || (gmax == best && G < winG)) {
                 best = gmax;
                 winG = G;
+                upd = true;
+                winL = l;
                 winP = gp;
             }
+        }
+
+        // A lane whose maximum moved to this multiplet recomputes the trials of the winning group's
+        // first maximal fine sample (or pair) from the levels still in shared memory, in the
+        // reference's order (fine time, then profile 0, 3l+1, 3l+2, 3l+3); the first equal to the
+        // maximum gives the output value and token.
+        if (__any_sync(0xffffffffu, upd)) {
+            if (upd) {
+                const int l = winL;
+                const int dt = g.dt[l], S = g.S[l], nsamp = g.nsamp[l];
+                const int j0 = g.I[l] + lane * nsamp;
+                const float w0 = (l == 0) ? wp[n] : 0.0f;
+                const float w1 = full ? wp[(3 * l + 1) * a.N + n] : 0.0f;
+                const float w2 = full ? wp[(3 * l + 2) * a.N + n] : 0.0f;
+                const float w3 = full ? wp[(3 * l + 3) * a.N + n] : 0.0f;
+                for (int is = winP; is < min(winP + 2, nsamp); is++) {
+                    const int j = j0 + is;
+                    const float x3 = lev[pf_phys(g, l, j)];
+                    const uint32_t tk0 = (uint32_t(m) << 16) | uint32_t(is * dt);
+                    if (l == 0) {
+                        const float v0 = __fmul_rn(w0, x3);
+                        if (v0 == best) { outv = v0; tok = tk0; break; }
+                    }
+                    if (full) {
+                        const float x0 = lev[pf_phys(g, l, j - 3 * S)];
+                        const float x1 = lev[pf_phys(g, l, j - 2 * S)];
+                        const float x2 = lev[pf_phys(g, l, j - S)];
+                        const float hx3 = __fmul_rn(0.5f, x3);
+                        const float v1 = __fmul_rn(w1, __fadd_rn(x2, x3));
+                        const float v2 = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3));
+                        const float v3 = __fmul_rn(w3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3));
+                        if (v1 == best) { outv = v1; tok = tk0 | (uint32_t(3 * l + 1) << 8); break; }
+                        if (v2 == best) { outv = v2; tok = tk0 | (uint32_t(3 * l + 2) << 8); break; }
+                        if (v3 == best) { outv = v3; tok = tk0 | (uint32_t(3 * l + 3) << 8); break; }
+                    }
+                }
+            }
+            __syncwarp();
         }
     }
 
     if (!active)
         return;
-
-    // Recompute the trials of the winning group's first maximal fine sample (or pair) in the
-    // reference's order; the first equal to the maximum wins.
-    float outv = best;
-    uint32_t tok = 0xffffffffu;
-    if (winG >= 0) {
-        const int l = winG / a.M, m = winG - l * a.M;
-        const int dt = g.dt[l], S = g.S[l], nsamp = g.nsamp[l];
-        const int n = a.m_to_n[m];
-        const float w0 = (l == 0) ? wp[n] : 0.0f;
-        const float w1 = full ? wp[(3 * l + 1) * a.N + n] : 0.0f;
-        const float w2 = full ? wp[(3 * l + 2) * a.N + n] : 0.0f;
-        const float w3 = full ? wp[(3 * l + 3) * a.N + n] : 0.0f;
-        const Ts *row = pfrows + (long) m * a.pf_cap;
-        const int j0 = g.I[l] + lane * nsamp;
-        for (int is = winP; is < min(winP + 2, nsamp); is++) {
-            const int j = j0 + is;
-            const float x3 = pf_tsum<Ts>(row, sbm, mask, j * dt, l);
-            const uint32_t tk0 = (uint32_t(m) << 16) | uint32_t(is * dt);
-            if (l == 0) {
-                const float v0 = __fmul_rn(w0, x3);
-                if (v0 == best) { outv = v0; tok = tk0; break; }
-            }
-            if (full) {
-                const float x0 = pf_tsum<Ts>(row, sbm, mask, (j - 3 * S) * dt, l);
-                const float x1 = pf_tsum<Ts>(row, sbm, mask, (j - 2 * S) * dt, l);
-                const float x2 = pf_tsum<Ts>(row, sbm, mask, (j - S) * dt, l);
-                const float hx3 = __fmul_rn(0.5f, x3);
-                const float v1 = __fmul_rn(w1, __fadd_rn(x2, x3));
-                const float v2 = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3));
-                const float v3 = __fmul_rn(w3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3));
-                if (v1 == best) { outv = v1; tok = tk0 | (uint32_t(3 * l + 1) << 8); break; }
-                if (v2 == best) { outv = v2; tok = tk0 | (uint32_t(3 * l + 2) << 8); break; }
-                if (v3 == best) { outv = v3; tok = tk0 | (uint32_t(3 * l + 3) << 8); break; }
-            }
-        }
-    }
     const long o = ((long) b * a.ndm_out + dm) * a.nt_out + tout;
     ((Ts *) a.out_max)[o] = from_f<Ts>(outv);
     a.out_argmax[o] = tok;
@@ -1162,7 +1191,7 @@ int pf_warp_floats(int Dout, int tpad, int Dcore, int L)
 }
 
 // Shared-memory layout of the fast peak finder for one warp (see PfGeom).
-static PfGeom pf_geom(int Dout, int Dcore, int tpad, int L)
+static PfGeom pf_geom(int Dout, int Dcore, int tpad, int L, int esize)
 {
     PfGeom g{};
     int off = 0;
@@ -1176,7 +1205,9 @@ static PfGeom pf_geom(int Dout, int Dcore, int tpad, int L)
         g.off[l] = off;
         g.e[l] = (nsamp - I % nsamp) % nsamp;
         g.k[l] = k;
-        g.pad[l] = pairs ? (nsamp >= 4 ? 2 : 0) : (nsamp >= 2 ? 1 : 0);
+        // Levels scanned in pairs from per-lane blocks: 2 floats after each block of >= 4 (the
+        // blocks then fall on distinct banks for 8-byte loads); the others are stored contiguously.
+        g.pad[l] = (pairs && nsamp >= 4) ? 2 : 0;
         g.I[l] = I;
         g.n[l] = 32 * nsamp + I;
         g.dt[l] = dt;
@@ -1193,7 +1224,9 @@ static PfGeom pf_geom(int Dout, int Dcore, int tpad, int L)
         const int size = t + g.pad[l] * (t >> k) + 1;
         off += (size + 1) & ~1;
     }
-    g.warp_floats = off;
+    g.raw_off = (off + 3) & ~3;
+    const int raw_floats = ((32 * Dout + tpad) * esize + 15) / 16 * 4;
+    g.warp_floats = g.raw_off + raw_floats;
     return g;
 }
 
@@ -1207,7 +1240,7 @@ template<typename Ts, int L>
 static void launch_pf_l(const PfArgs &a, int B, cudaStream_t s)
 {
     if (pf_fast_ok(a)) {
-        const PfGeom g = pf_geom(a.Dout, a.Dcore, a.tpad, L);
+        const PfGeom g = pf_geom(a.Dout, a.Dcore, a.tpad, L, (int) sizeof(Ts));
         size_t sm = (size_t) kPfWarps * g.warp_floats * sizeof(float);
         set_smem(pf_fast_kernel<Ts, L>, sm);
         dim3 grid((a.nt_out + 31) / 32, (a.ndm_out + kPfWarps - 1) / kPfWarps, B);
