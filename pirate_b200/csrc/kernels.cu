@@ -364,36 +364,44 @@ struct PfEmit
     }
 };
 
-// Shared-memory delay line between the phases: row rr = f * 2^RA + d (f < 2^RB) has capacity
-// P(f, d) + 64. Phase a writes tile k at wpos while phase b reads tile k-1 at rpos - P.
-struct RingTab
-{
-    int *off, *cap, *wpos, *rpos;
-};
-
+// Shared-memory delay line between the phases: row rr = f * 2^RA + d (f < 2^RB) starts at float
+// off(rr) and has capacity cap(rr) = ring_cap(f, d), a multiple of 32. Phase a writes tile k at
+// wpos, phase b reads tile k-1 at rpos - P(f, d); positions are multiples of 32, so a write never
+// wraps and a read wraps at most once. Per row the tables hold
+//   wb[rr] = off + wpos                          (phase a: write index of lane 0)
+//   rt[rr] = {off + rpos - P, off, cap, off + cap - P}   (phase b: read index of lane 0, wrap bounds)
 template<int RA, int RB>
 __device__ __forceinline__ int ring_lag(int f, int d) { return ((1 << RB) - 1 - f) * brev_bits(d, RA); }
 
 __device__ __forceinline__ int wrap_add(int p, int cap) { return (p >= cap) ? (p - cap) : ((p < 0) ? (p + cap) : p); }
 
+// Fills wb[] and rt[] for stream time s0 (a multiple of 32). Uses ioff[NR] as scratch; ends with
+// __syncthreads().
 template<int RA, int RB>
-__device__ void ring_init(RingTab &t, int *sm_int, long s0)
+__device__ void ring_init(int *wb, int4 *rt, int *ioff, long s0)
 {
     constexpr int NR = 1 << (RA + RB);
-    t.off = sm_int;
-    t.cap = sm_int + NR;
-    t.wpos = sm_int + 2 * NR;
-    t.rpos = sm_int + 3 * NR;
+    const int rr = threadIdx.x;
+    const int f = rr >> RA, d = rr & ((1 << RA) - 1);
+    if (rr < NR)
+        ioff[rr] = ring_cap(RA, RB, f, d);
+    __syncthreads();
     if (threadIdx.x == 0) {
         int o = 0;
-        for (int rr = 0; rr < NR; rr++) {
-            int c = ring_lag<RA, RB>(rr >> RA, rr & ((1 << RA) - 1)) + 64;
-            t.off[rr] = o;
-            t.cap[rr] = c;
-            t.wpos[rr] = t.rpos[rr] = int(s0 % c);
+        for (int i = 0; i < NR; i++) {
+            const int c = ioff[i];
+            ioff[i] = o;
             o += c;
         }
     }
+    __syncthreads();
+    if (rr < NR) {
+        const int off = ioff[rr], cap = ring_cap(RA, RB, f, d), P = ring_lag<RA, RB>(f, d);
+        const int pos = int(s0 % cap);
+        wb[rr] = off + pos;
+        rt[rr] = make_int4(off + pos - P, off, cap, off + cap - P);
+    }
+    __syncthreads();
 }
 
 __device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
@@ -419,6 +427,23 @@ template<typename Ts> struct Stage
     static constexpr int SPR = (sizeof(Ts) == 4) ? 32 : 34;   // samples per row
 };
 
+// Shared-memory layout of a two-phase tree kernel (byte offsets; host and device agree).
+template<typename Ts, int RA, int RB>
+struct TreeSmem
+{
+    static constexpr int NR = 1 << (RA + RB);
+    static constexpr size_t in_off = 0;                       // long[NR]
+    static constexpr size_t out_base = in_off + 8 * NR;       // long[NR]
+    static constexpr size_t out_off = out_base + 8 * NR;      // long[NR]
+    static constexpr size_t rt = out_off + 8 * NR;            // int4[NR]
+    static constexpr size_t wb = rt + 16 * NR;                // int[NR]
+    static constexpr size_t in_pos = wb + 4 * NR;             // int[NR]
+    static constexpr size_t in_cap = in_pos + 4 * NR;         // int[NR]
+    static constexpr size_t staging = (in_cap + 4 * NR + 15) & ~size_t(15);
+    static constexpr size_t ring = (staging + 2 * (1 << RB) * (1 << RA) * Stage<Ts>::SPR * sizeof(Ts) + 15) & ~size_t(15);
+    static constexpr size_t total = ring + sizeof(float) * ring_floats(RA, RB);
+};
+
 template<int STAGE>
 struct TreeArgsOf;
 template<> struct TreeArgsOf<1> { using type = Stage1Args; };
@@ -433,43 +458,42 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
 {
     constexpr int NA = 1 << RA, NB = 1 << RB, NR = 1 << (RA + RB);
     constexpr int RING = ring_floats(RA, RB);
-    // Stage-1 rows are read aligned (32 samples = 16 words for 16-bit storage); stage-2 rows start at
-    // an arbitrary sample and need one extra word. Copying the extra word for aligned rows would read
-    // past the end of the last row's buffer.
-    constexpr int WPR = (STAGE == 1 && sizeof(Ts) != 4) ? 16 : Stage<Ts>::WPR;
-    constexpr int SPR = Stage<Ts>::SPR;
-    extern __shared__ long long sm_ll[];
+    constexpr int WPR = Stage<Ts>::WPR;   // stage 2: 4-byte words copied per row and tile
+    // Staging row stride: stage-1 rows are 32 aligned samples (16-byte copies); stage-2 rows start at
+    // an arbitrary sample and take one extra 16-bit sample.
+    constexpr int SPRK = (STAGE == 1) ? 32 : Stage<Ts>::SPR;
+    using Lay = TreeSmem<Ts, RA, RB>;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
 
-    // Shared layout: [in_off (NR longs) | ring tables 4*NR ints | in_pos, in_cap, out_pos NR ints each |
-    //                 staging 2 x NB x NA x SPR | ring RING floats]
-    long *in_off = (long *) sm_ll;
-    long *out_off = in_off + NR;                    // stage 1: offsets of the output delay lines
-    int *sm_int = (int *) (out_off + NR);
-    RingTab tab;
-    int *in_pos = sm_int + 4 * NR;
-    int *in_cap = in_pos + NR;
-    int *out_pos = in_cap + NR;
-    Ts *staging = (Ts *) (out_pos + NR);
-    float *ring = (float *) (staging + 2 * NB * NA * SPR);
-    ring = (float *) (((uintptr_t) ring + 15) & ~uintptr_t(15));
+    long *in_off = (long *) (sm_raw + Lay::in_off);       // stage 2: input delay line offsets
+    long *out_base = (long *) (sm_raw + Lay::out_base);   // stage 1: output delay line index of lane 0
+    long *out_off = (long *) (sm_raw + Lay::out_off);     // stage 1: output delay line offsets
+    int4 *rt = (int4 *) (sm_raw + Lay::rt);
+    int *wb = (int *) (sm_raw + Lay::wb);
+    int *in_pos = (int *) (sm_raw + Lay::in_pos);         // stage 2: input read positions
+    int *in_cap = (int *) (sm_raw + Lay::in_cap);         // stage 2: input capacities; stage 1: output capacities
+    Ts *staging = (Ts *) (sm_raw + Lay::staging);
+    float *ring = (float *) (sm_raw + Lay::ring);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
     float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
 
-    ring_init<RA, RB>(tab, sm_int, a.s0);
+    ring_init<RA, RB>(wb, rt, in_cap, a.s0);
     for (int i = threadIdx.x; i < RING; i += blockDim.x)
         ring[i] = st[i];
 
     const Ts *in;
+    int pos1 = 0;   // stage 1: read position of every input row (rows are read aligned)
     if constexpr (STAGE == 1) {
-        in = (const Ts *) a.in + (long) (a.in_beam0 + b) * a.in_beam_stride;
+        in = (const Ts *) a.in + (long) (a.in_beam0 + b) * a.in_beam_stride + (long) blk * NR * a.in_row_stride;
+        pos1 = int(a.in_s0 & a.in_mask);
         for (int r = threadIdx.x; r < NR; r += blockDim.x) {
-            in_off[r] = ((long) blk * NR + r) * a.in_row_stride;
-            in_pos[r] = int(a.in_s0 & a.in_mask);
-            in_cap[r] = a.ring_cap[(long) blk * NR + r];   // stage 1: capacity of output delay line r
-            out_off[r] = a.ring_off[(long) blk * NR + r];
-            out_pos[r] = int(a.s0 % in_cap[r]);
+            const int cap = a.ring_cap[(long) blk * NR + r];   // capacity of output delay line r (a multiple of 32)
+            const long off = a.ring_off[(long) blk * NR + r];
+            in_cap[r] = cap;
+            out_off[r] = off;
+            out_base[r] = off + a.s0 % cap;
         }
     } else {
         in = (const Ts *) a.ring + (long) bt * a.ring_beam_stride;
@@ -499,28 +523,39 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
 
         // Issues the cp.async copies of this warp's NA rows for one tile into staging buffer 'buf',
         // then advances the rows' read positions by 32 samples.
-        Ts *my_stage = staging + g * NA * SPR;
+        Ts *my_stage = staging + g * NA * SPRK;
         auto issue = [&](int buf) {
-            Ts *dst = my_stage + buf * NB * NA * SPR;
-            for (int idx = lane; idx < NA * WPR; idx += 32) {
-                const int i = idx / WPR, w = idx - i * WPR;
-                const int r = g * NA + i;
-                int p = in_pos[r];
-                const Ts *src;
-                if constexpr (STAGE == 1) {
-                    src = in + in_off[r] + ((sizeof(Ts) == 4) ? (p + w) : (p + 2 * w));
-                } else {
-                    int c = in_cap[r];
-                    int q = (sizeof(Ts) == 4) ? wrap_add(p + w, c) : wrap_add((p & ~1) + 2 * w, c);
-                    src = in + in_off[r] + q;
+            Ts *dst = my_stage + buf * NB * NA * SPRK;
+            if constexpr (STAGE == 1) {
+                // Aligned rows at a common position: 16-byte copies, CH per row.
+                constexpr int EPC = 16 / sizeof(Ts), CH = 32 / EPC;
+                for (int c = lane; c < NA * CH; c += 32) {
+                    const int i = c / CH, k = c % CH;
+                    cp_async_bytes<16>(dst + i * SPRK + k * EPC, in + (long) (g * NA + i) * a.in_row_stride + pos1 + k * EPC);
                 }
-                cp_async4(dst + i * SPR + ((sizeof(Ts) == 4) ? w : 2 * w), src);
-            }
-            __syncwarp();
-            if (lane < NA) {
-                const int r = g * NA + lane;
-                if constexpr (STAGE == 1) in_pos[r] = int((in_pos[r] + 32) & a.in_mask);
-                else in_pos[r] = wrap_add(in_pos[r] + 32, in_cap[r]);
+                pos1 = int((pos1 + 32) & a.in_mask);
+            } else {
+                // Rows at their own positions, in 4-byte words (LPR lanes per row, WPL words each);
+                // a word wraps the delay line at most once.
+                constexpr int LPR = 32 / NA, WPL = (WPR + LPR - 1) / LPR;
+                const int i = lane / LPR, r = g * NA + i, w0 = (lane % LPR) * WPL;
+                const int p = in_pos[r], c = in_cap[r];
+                const Ts *row = in + in_off[r];
+                Ts *d = dst + i * SPRK;
+#pragma unroll
+                for (int u = 0; u < WPL; u++) {
+                    const int w = w0 + u;
+                    if (w < WPR) {
+                        int q = (sizeof(Ts) == 4) ? (p + w) : ((p & ~1) + 2 * w);
+                        q = (q >= c) ? (q - c) : q;
+                        cp_async4(d + ((sizeof(Ts) == 4) ? w : 2 * w), row + q);
+                    }
+                }
+                __syncwarp();
+                if (lane < NA) {
+                    const int rr = g * NA + lane;
+                    in_pos[rr] = wrap_add(in_pos[rr] + 32, in_cap[rr]);
+                }
             }
             __syncwarp();
         };
@@ -539,20 +574,20 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 cp_async_commit();
                 cp_async_wait1();
                 __syncwarp();
-                const Ts *sb = my_stage + (it & 1) * NB * NA * SPR;
+                const Ts *sb = my_stage + (it & 1) * NB * NA * SPRK;
                 float v[NA];
 #pragma unroll
-                for (int i = 0; i < NA; i++) v[i] = to_f(sb[i * SPR + lane + ((par >> i) & 1)]);
+                for (int i = 0; i < NA; i++) v[i] = to_f(sb[i * SPRK + lane + ((par >> i) & 1)]);
                 rt_steps<RA>(v, pva, lane);
 #pragma unroll
-                for (int i = 0; i < NA; i++) {
-                    const int rr = g * NA + i;
-                    ring[tab.off[rr] + wrap_add(tab.wpos[rr] + lane, tab.cap[rr])] = v[i];
-                }
+                for (int i = 0; i < NA; i++)
+                    ring[wb[g * NA + i] + lane] = v[i];
                 __syncwarp();
                 if (lane < NA) {
                     const int rr = g * NA + lane;
-                    tab.wpos[rr] = wrap_add(tab.wpos[rr] + 32, tab.cap[rr]);
+                    const int lo = rt[rr].y, cap = rt[rr].z;   // phase b updates only rt[].x
+                    const int w = wb[rr] + 32;
+                    wb[rr] = (w == lo + cap) ? lo : w;
                 }
             }
             asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
@@ -580,26 +615,29 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 float v[NB];
 #pragma unroll
                 for (int f = 0; f < NB; f++) {
-                    const int rr = f * NA + g;
-                    v[f] = ring[tab.off[rr] + wrap_add(tab.rpos[rr] + lane - ring_lag<RA, RB>(f, g), tab.cap[rr])];
+                    const int4 t = rt[f * NA + g];
+                    int q = t.x + lane;
+                    q = (q < t.y) ? (q + t.z) : q;
+                    v[f] = ring[q];
                 }
                 __syncwarp();
                 if (lane < NB) {
                     const int rr = lane * NA + g;
-                    tab.rpos[rr] = wrap_add(tab.rpos[rr] + 32, tab.cap[rr]);
+                    const int4 t = rt[rr];
+                    const int x = t.x + 32;
+                    rt[rr].x = (x >= t.w) ? (x - t.z) : x;
                 }
                 if constexpr (STAGE == 1) {
                     rt_steps<RB>(v, pvb, lane);
                     Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride;
 #pragma unroll
-                    for (int f = 0; f < NB; f++) {
-                        const int i = (f << RA) | g;
-                        out[out_off[i] + wrap_add(out_pos[i] + lane, in_cap[i])] = from_f<Ts>(v[f]);
-                    }
+                    for (int f = 0; f < NB; f++)
+                        out[out_base[(f << RA) | g] + lane] = from_f<Ts>(v[f]);
                     __syncwarp();
                     if (lane < NB) {
                         const int i = (lane << RA) | g;
-                        out_pos[i] = wrap_add(out_pos[i] + 32, in_cap[i]);
+                        const long ob = out_base[i] + 32;
+                        out_base[i] = (ob == out_off[i] + in_cap[i]) ? out_off[i] : ob;
                     }
                 } else {
                     emit.s = a.s0 + (long) tile * 32 + lane;
@@ -1119,9 +1157,7 @@ void launch_grid_lds(const GridLdsArgs &a, int dtype, cudaStream_t s)
 template<typename Ts, int RA, int RB>
 static size_t tree_smem()
 {
-    constexpr int NR = 1 << (RA + RB);
-    return (size_t) 2 * NR * 8 + 7 * NR * 4 + 2 * (1 << RB) * (1 << RA) * Stage<Ts>::SPR * sizeof(Ts) + 16
-           + (size_t) ring_floats(RA, RB) * sizeof(float);
+    return TreeSmem<Ts, RA, RB>::total;
 }
 
 template<typename K>

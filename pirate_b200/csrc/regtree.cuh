@@ -76,13 +76,18 @@ __host__ __device__ constexpr int st_off(int K, int r0, int u0)
     return s;
 }
 
-// Floats of delay line between the phases: row (f, d) holds P(f, d) + 64 samples (phase a writes
-// tile k while phase b reads tile k-1).
+// Delay line between the phases: row (f, d) holds P(f, d) + 64 samples (phase a writes tile k while
+// phase b reads tile k-1), rounded up to a multiple of 32 so that a tile never wraps on write.
+__host__ __device__ constexpr int ring_cap(int RA, int RB, int f, int d)
+{
+    return (((1 << RB) - 1 - f) * bitrev_c(d, RA) + 64 + 31) & ~31;
+}
+
 __host__ __device__ constexpr int ring_floats(int RA, int RB)
 {
     int s = 0;
     for (int f = 0; f < (1 << RB); f++)
-        for (int d = 0; d < (1 << RA); d++) s += ((1 << RB) - 1 - f) * bitrev_c(d, RA) + 64;
+        for (int d = 0; d < (1 << RA); d++) s += ring_cap(RA, RB, f, d);
     return s;
 }
 
