@@ -17,7 +17,9 @@ import numpy as np
 __all__ = ["DedispersionConfig", "DedispersionPlan", "GpuDedisperser", "Outputs", "lib", "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libpirate_b200.so")
+# The in-tree build; PB2_LIBRARY names another build of the same library (for example one made with
+# different compile options) to load instead.
+LIB_PATH = os.environ.get("PB2_LIBRARY") or os.path.join(HERE, "libpirate_b200.so")
 MAX_TREES = 64
 
 _lib = None

@@ -211,10 +211,27 @@ template<int K> struct RT
     static constexpr int NS = (K > 0) ? K : 1;
 };
 
-// All K steps of a register tree, in place. pv[r][q] holds pair q's row0 input of the previous tile.
-template<int K>
-__device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>::NS][RT<K>::NP], int lane)
+// Butterfly of a lag-0 pair whose history (the previous tile's row0 at lane 31, the only lane that
+// needs it) lives in shared memory at *h instead of a register: lane 0 takes it for the lag-1
+// operand, then lane 31 stores this tile's row0. The load precedes the store in the warp's program
+// order, and the loop's __syncwarp() orders the store before the next tile's load.
+__device__ __forceinline__ void bfly_l0_shared(float &v0, float &v1, float *h, int lane)
 {
+    const float x = v0, y = v1, hp = *h;
+    float b = __shfl_sync(kFull, x, lane - 1);
+    b = (lane == 0) ? hp : b;
+    v0 = bfly(x, y);
+    v1 = bfly(b, y);
+    if (lane == 31) *h = x;
+}
+
+// All K steps of a register tree, in place. pv[r][q] holds pair q's row0 input of the previous tile.
+// With HS, the lag-0 pairs keep that history in shared memory (hs[slot], one float per pair, in
+// (r, q) order), which frees their registers.
+template<int K, bool HS = false>
+__device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>::NS][RT<K>::NP], int lane, float *hs = nullptr)
+{
+    int slot = 0;
 #pragma unroll
     for (int r = 0; r < K; r++) {
 #pragma unroll
@@ -222,6 +239,11 @@ __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>
             const int h = 1 << r;
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
             const int L = rt_lag(r, q);
+            if (HS && L == 0) {
+                bfly_l0_shared(v[i0], v[i0 + h], hs + slot, lane);
+                slot++;
+                continue;
+            }
             float x = v[i0], y = v[i0 + h];
             float a = (L == 0) ? x : lagged(x, pv[r][q], L, lane);
             float b = lagged(x, pv[r][q], L + 1, lane);
@@ -233,32 +255,45 @@ __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>
 }
 
 // Persistent histories: pair (r, q) needs its previous-tile row0 only in lanes >= 31 - lag.
-template<int K>
-__device__ __forceinline__ void rt_load(float (&pv)[RT<K>::NS][RT<K>::NP], const float *st, int lane)
+// With HS the lag-0 pairs' single value goes to or comes from hs[slot].
+template<int K, bool HS = false>
+__device__ __forceinline__ void rt_load(float (&pv)[RT<K>::NS][RT<K>::NP], const float *st, int lane, float *hs = nullptr)
 {
-    int off = 0;
+    int off = 0, slot = 0;
 #pragma unroll
     for (int r = 0; r < K; r++)
 #pragma unroll
         for (int q = 0; q < RT<K>::NP; q++) {
             const int L = rt_lag(r, q);
-            int i = lane - (31 - L);
-            pv[r][q] = (i >= 0) ? st[off + i] : 0.0f;
+            if (HS && L == 0) {
+                if (lane == 0) hs[slot] = st[off];
+                slot++;
+            } else {
+                int i = lane - (31 - L);
+                pv[r][q] = (i >= 0) ? st[off + i] : 0.0f;
+            }
             off += L + 1;
         }
+    if (HS) __syncwarp();
 }
 
-template<int K>
-__device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP], float *st, int lane)
+template<int K, bool HS = false>
+__device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP], float *st, int lane, const float *hs = nullptr)
 {
-    int off = 0;
+    if (HS) __syncwarp();
+    int off = 0, slot = 0;
 #pragma unroll
     for (int r = 0; r < K; r++)
 #pragma unroll
         for (int q = 0; q < RT<K>::NP; q++) {
             const int L = rt_lag(r, q);
-            int i = lane - (31 - L);
-            if (i >= 0) st[off + i] = pv[r][q];
+            if (HS && L == 0) {
+                if (lane == 0) st[off] = hs[slot];
+                slot++;
+            } else {
+                int i = lane - (31 - L);
+                if (i >= 0) st[off + i] = pv[r][q];
+            }
             off += L + 1;
         }
 }
@@ -267,12 +302,13 @@ __device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP],
 // pf level r'+1 are emitted (FrequencySubbands multiplet order), reproducing ReferenceTree::dedisperse_2d
 // (src_lib/ReferenceTree.cpp:120-300): even band pairs coincide with the in-place butterflies, odd
 // ("staggered") pairs (2k+1, 2k+2) are extra butterflies with their own histories ps[r'][u].
-template<int RB, bool STAG, typename Emit>
+template<int RB, bool STAG, bool HS, typename Emit>
 __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv)[RT<RB>::NS][RT<RB>::NP],
                                                  float (&ps)[RT<RB>::NS][RT<RB>::NP], const Stage2Args &a,
-                                                 int lane, Emit emit)
+                                                 int lane, Emit emit, float *hs)
 {
     constexpr int NB = 1 << RB;
+    int slot = 0;   // HS: lag-0 in-place pairs keep their history in hs[slot] (see rt_steps)
 #pragma unroll
     for (int f = 0; f < NB; f++)
         if (f < a.sb_count[0]) emit(a.sb_mbase[0] + f, v[f]);
@@ -301,13 +337,18 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
             const int k = q >> r, j = q & (h - 1);
             const int L = rt_lag(r, q);
-            float x = v[i0], y = v[i0 + h];
-            float aa = (L == 0) ? x : lagged(x, pv[r][q], L, lane);
-            float bb = lagged(x, pv[r][q], L + 1, lane);
-            float o0 = bfly(aa, y), o1 = bfly(bb, y);
-            v[i0] = o0;
-            v[i0 + h] = o1;
-            pv[r][q] = x;
+            if (HS && L == 0) {
+                bfly_l0_shared(v[i0], v[i0 + h], hs + slot, lane);
+                slot++;
+            } else {
+                float x = v[i0], y = v[i0 + h];
+                float aa = (L == 0) ? x : lagged(x, pv[r][q], L, lane);
+                float bb = lagged(x, pv[r][q], L + 1, lane);
+                v[i0] = bfly(aa, y);
+                v[i0 + h] = bfly(bb, y);
+                pv[r][q] = x;
+            }
+            const float o0 = v[i0], o1 = v[i0 + h];
             if (2 * k < cnt) {
                 int m = mb + (2 * k) * (2 << r) + 2 * bitrev_c(j, r);
                 emit(m, o0);
@@ -356,11 +397,11 @@ __device__ __forceinline__ void st_save(const float (&ps)[RT<K>::NS][RT<K>::NP],
 template<typename Ts>
 struct PfEmit
 {
-    Ts *pf;
-    long rowbase, cap, mask, s;
+    Ts *row0;   // multiplet 0 of this warp's coarse dm, at the current tile's slot + lane
+    int cap;    // delay line capacity (multiplet stride)
     __device__ __forceinline__ void operator()(int m, float v) const
     {
-        pf[(rowbase + m) * cap + (s & mask)] = from_f<Ts>(v);
+        row0[m * cap] = from_f<Ts>(v);
     }
 };
 
@@ -404,11 +445,6 @@ __device__ void ring_init(int *wb, int4 *rt, int *ioff, long s0)
     __syncthreads();
 }
 
-__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
-{
-    unsigned s = (unsigned) __cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" :: "r"(s), "l"(gmem) : "memory");
-}
 template<int BYTES>
 __device__ __forceinline__ void cp_async_bytes(void *smem, const void *gmem)
 {
@@ -421,10 +457,13 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 
 // Staging of one tile of a phase-a warp's NA input rows: 32-bit words copied with cp.async.
 // float: 32 words per row; 16-bit types: 17 words (34 samples) starting at an even sample.
+// Staging of one tile of input rows with 16-byte cp.async copies of EPC samples. Stage-1 rows are
+// read aligned (32 samples); a stage-2 row starts at an arbitrary sample p and is copied as the
+// EPC-aligned run of 32 + EPC samples from p & ~(EPC-1) (SPR samples per staged row).
 template<typename Ts> struct Stage
 {
-    static constexpr int WPR = (sizeof(Ts) == 4) ? 32 : 17;   // words per row
-    static constexpr int SPR = (sizeof(Ts) == 4) ? 32 : 34;   // samples per row
+    static constexpr int EPC = 16 / sizeof(Ts);
+    static constexpr int SPR = 32 + EPC;
 };
 
 // Shared-memory layout of a two-phase tree kernel (byte offsets; host and device agree).
@@ -439,10 +478,15 @@ struct TreeSmem
     static constexpr size_t wb = rt + 16 * NR;                // int[NR]
     static constexpr size_t in_pos = wb + 4 * NR;             // int[NR]
     static constexpr size_t in_cap = in_pos + 4 * NR;         // int[NR]
-    static constexpr size_t staging = (in_cap + 4 * NR + 15) & ~size_t(15);
+    static constexpr size_t hist = in_cap + 4 * NR;           // float[warps][16]: lag-0 histories
+    static constexpr size_t staging = (hist + 4 * 16 * ((1 << RA) + (1 << RB)) + 15) & ~size_t(15);
     static constexpr size_t ring = (staging + 2 * (1 << RB) * (1 << RA) * Stage<Ts>::SPR * sizeof(Ts) + 15) & ~size_t(15);
     static constexpr size_t total = ring + sizeof(float) * ring_floats(RA, RB);
 };
+
+// Lag-0 histories in shared memory (HS in rt_steps) for the rank-7 and rank-8 trees, whose register
+// budgets (64 and 80 per thread in 1024- and 768-thread blocks) are the tightest.
+__host__ __device__ constexpr bool tree_hs(int RA, int RB, int STAGE) { return RA + RB >= 7; }
 
 template<int STAGE>
 struct TreeArgsOf;
@@ -453,14 +497,12 @@ template<> struct TreeArgsOf<2> { using type = Stage2Args; };
 // tile k-1; one block barrier per tile.
 //   STAGE 1: input = level-p tree rows (aligned), output = per-row stage-1 delay lines.
 //   STAGE 2: input = stage-1 delay lines read at lag rb_lag (misaligned), output = subband rows.
-template<typename Ts, int RA, int RB, int STAGE, bool STAG>
+template<typename Ts, int RA, int RB, int STAGE, bool STAG, bool HS = tree_hs(RA, RB, STAGE)>
 __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(typename TreeArgsOf<STAGE>::type a)
 {
     constexpr int NA = 1 << RA, NB = 1 << RB, NR = 1 << (RA + RB);
     constexpr int RING = ring_floats(RA, RB);
-    constexpr int WPR = Stage<Ts>::WPR;   // stage 2: 4-byte words copied per row and tile
-    // Staging row stride: stage-1 rows are 32 aligned samples (16-byte copies); stage-2 rows start at
-    // an arbitrary sample and take one extra 16-bit sample.
+    // Staging row stride: stage-1 rows are 32 aligned samples; stage-2 rows take one more chunk.
     constexpr int SPRK = (STAGE == 1) ? 32 : Stage<Ts>::SPR;
     using Lay = TreeSmem<Ts, RA, RB>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -476,6 +518,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     float *ring = (float *) (sm_raw + Lay::ring);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *hs = (float *) (sm_raw + Lay::hist) + warp * 16;   // this warp's lag-0 histories (HS)
     const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
     float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
 
@@ -519,7 +562,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     if (is_a) {
         float pva[RT<RA>::NS][RT<RA>::NP];
         float *sta = st + RING + g * rt_state(RA);
-        rt_load<RA>(pva, sta, lane);
+        rt_load<RA, HS>(pva, sta, lane, hs);
 
         // Issues the cp.async copies of this warp's NA rows for one tile into staging buffer 'buf',
         // then advances the rows' read positions by 32 samples.
@@ -535,21 +578,16 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 }
                 pos1 = int((pos1 + 32) & a.in_mask);
             } else {
-                // Rows at their own positions, in 4-byte words (LPR lanes per row, WPL words each);
-                // a word wraps the delay line at most once.
-                constexpr int LPR = 32 / NA, WPL = (WPR + LPR - 1) / LPR;
-                const int i = lane / LPR, r = g * NA + i, w0 = (lane % LPR) * WPL;
-                const int p = in_pos[r], c = in_cap[r];
-                const Ts *row = in + in_off[r];
-                Ts *d = dst + i * SPRK;
-#pragma unroll
-                for (int u = 0; u < WPL; u++) {
-                    const int w = w0 + u;
-                    if (w < WPR) {
-                        int q = (sizeof(Ts) == 4) ? (p + w) : ((p & ~1) + 2 * w);
-                        q = (q >= c) ? (q - c) : q;
-                        cp_async4(d + ((sizeof(Ts) == 4) ? w : 2 * w), row + q);
-                    }
+                // Rows at their own positions: CPR consecutive 16-byte chunks from p & ~(EPC-1), consecutive
+                // lanes on consecutive chunks of a row. Capacities are multiples of 32 samples, so a chunk
+                // never straddles the end of a delay line and wraps at most once.
+                constexpr int EPC = Stage<Ts>::EPC, CPR = 32 / EPC + 1;
+                for (int c = lane; c < NA * CPR; c += 32) {
+                    const int i = c / CPR, k = c - i * CPR, r = g * NA + i;
+                    const int cap = in_cap[r];
+                    int q = (in_pos[r] & ~(EPC - 1)) + k * EPC;
+                    q = (q >= cap) ? (q - cap) : q;
+                    cp_async_bytes<16>(dst + i * SPRK + k * EPC, in + in_off[r] + q);
                 }
                 __syncwarp();
                 if (lane < NA) {
@@ -560,10 +598,14 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
             __syncwarp();
         };
 
-        unsigned par = 0;   // stage 2, 16-bit storage: bit i = sample parity of row i (constant: capacities are even)
-        if (STAGE == 2 && sizeof(Ts) != 4) {
+        // Stage 2: bits [OB i, OB i + OB) = offset of row i's first sample in its staged run,
+        // p & (EPC-1) (constant: positions advance by 32 and capacities are multiples of 32).
+        constexpr int OB = (sizeof(Ts) == 4) ? 2 : 3;
+        unsigned long long offs = 0;
+        if (STAGE == 2) {
 #pragma unroll
-            for (int i = 0; i < NA; i++) par |= unsigned(in_pos[g * NA + i] & 1) << i;
+            for (int i = 0; i < NA; i++)
+                offs |= (unsigned long long) (in_pos[g * NA + i] & (Stage<Ts>::EPC - 1)) << (OB * i);
         }
         issue(0);
         cp_async_commit();
@@ -577,8 +619,9 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 const Ts *sb = my_stage + (it & 1) * NB * NA * SPRK;
                 float v[NA];
 #pragma unroll
-                for (int i = 0; i < NA; i++) v[i] = to_f(sb[i * SPRK + lane + ((par >> i) & 1)]);
-                rt_steps<RA>(v, pva, lane);
+                for (int i = 0; i < NA; i++)
+                    v[i] = to_f(sb[i * SPRK + lane + int((offs >> (OB * i)) & ((1u << OB) - 1))]);
+                rt_steps<RA, HS>(v, pva, lane, hs);
 #pragma unroll
                 for (int i = 0; i < NA; i++)
                     ring[wb[g * NA + i] + lane] = v[i];
@@ -593,25 +636,26 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
             asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
         }
         cp_async_wait0();
-        rt_save<RA>(pva, sta, lane);
+        rt_save<RA, HS>(pva, sta, lane, hs);
     } else {
         float pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
         float *stb = st + RING + NB * rt_state(RA) + g * (rt_state(RB) + (STAGE == 2 ? st_state(RB) : 0));
-        rt_load<RB>(pvb, stb, lane);
+        rt_load<RB, HS>(pvb, stb, lane, hs);
         if (STAG) st_load<RB>(psb, stb + rt_state(RB), lane);
 
         PfEmit<Ts> emit;
+        Ts *pf_rows = nullptr;   // stage 2: multiplet 0 of this warp's coarse dm
+        int pf_slot = 0;         // stage 2: delay-line slot of this lane's sample in the current tile
         if constexpr (STAGE == 2) {
-            emit.pf = (Ts *) a.pf;
-            emit.cap = a.pf_cap;
-            emit.mask = a.pf_cap - 1;
             const int pf_dm = brev_bits(g, RA);
-            emit.rowbase = ((long) bt * a.ndm_out + ((long) brev_bits(blk, a.amb_rank) << RA) + pf_dm) * a.M;
+            const long rowbase = ((long) bt * a.ndm_out + ((long) brev_bits(blk, a.amb_rank) << RA) + pf_dm) * a.M;
+            pf_rows = (Ts *) a.pf + rowbase * a.pf_cap;
+            pf_slot = int((a.s0 + lane) & (a.pf_cap - 1));
+            emit.cap = int(a.pf_cap);
         }
 
         for (int it = 0; it <= ntiles; it++) {
             if (it >= 1) {
-                const int tile = it - 1;
                 float v[NB];
 #pragma unroll
                 for (int f = 0; f < NB; f++) {
@@ -628,7 +672,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                     rt[rr].x = (x >= t.w) ? (x - t.z) : x;
                 }
                 if constexpr (STAGE == 1) {
-                    rt_steps<RB>(v, pvb, lane);
+                    rt_steps<RB, HS>(v, pvb, lane, hs);
                     Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride;
 #pragma unroll
                     for (int f = 0; f < NB; f++)
@@ -640,13 +684,14 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                         out_base[i] = (ob == out_off[i] + in_cap[i]) ? out_off[i] : ob;
                     }
                 } else {
-                    emit.s = a.s0 + (long) tile * 32 + lane;
-                    phase_b_subbands<RB, STAG>(v, pvb, psb, a, lane, emit);
+                    emit.row0 = pf_rows + pf_slot;
+                    pf_slot = (pf_slot + 32) & int(a.pf_cap - 1);
+                    phase_b_subbands<RB, STAG, HS>(v, pvb, psb, a, lane, emit, hs);
                 }
             }
             asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
         }
-        rt_save<RB>(pvb, stb, lane);
+        rt_save<RB, HS>(pvb, stb, lane, hs);
         if (STAG) st_save<RB>(psb, stb + rt_state(RB), lane);
     }
     __syncthreads();
