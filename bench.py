@@ -63,22 +63,30 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []          # (host time, csv line)
+        self.window = None       # (start, end) host times of the timed region
 
     def __enter__(self):
+        """Starts sampling every 50 ms and waits (up to 3 s) for the first sample."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, start, end):
+        self.window = (start, end)
 
     def __exit__(self, *a):
         if self.proc:
@@ -91,7 +99,15 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines
+        if self.window:
+            # samples taken during the timed region (the one just after it if the region was shorter
+            # than the sampling interval)
+            inside = [ln for t, ln in lines if self.window[0] <= t <= self.window[1] + 0.06]
+            lines = inside or [ln for t, ln in lines if t >= self.window[0]][:1]
+        else:
+            lines = [ln for _, ln in lines]
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
@@ -158,11 +174,13 @@ def run_ours(args, rank, world):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clk:
+        h0 = time.time()
         e0.record(stream)
         for _ in range(args.steps):
             step_device()
         e1.record(stream)
         torch.cuda.synchronize()
+        clk.mark(h0, time.time())
     ktimes = dd.kernel_times()
     dd.enable_timing(False)
     ms = e0.elapsed_time(e1)
@@ -279,7 +297,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--beams", type=int, default=4)
     ap.add_argument("--dtype", default="float16", choices=["float16", "bfloat16", "float32"])
@@ -343,14 +361,18 @@ def main():
     dom_launches_per_step = kt[dom][1] / nsteps
     dom_bytes = r["alg"][classes.index(dom)]
     achieved = dom_bytes / (dom_ms_per_step * 1e-3) / 1e9
+    # DRAM traffic per launch of the dominant kernel: the ncu-measured ratio of DRAM bytes
+    # (dram__bytes_read.sum + dram__bytes_write.sum) to algorithmic bytes on a capture of the same
+    # kernel, times this workload's algorithmic bytes per launch (profiles/traffic.json).
     traffic = None
+    dom_bytes_per_launch = dom_bytes / dom_launches_per_step if dom_launches_per_step else None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and dom_bytes_per_launch:
         try:
             with open(tpath) as f:
                 tj = json.load(f)
-            if dom in tj and tj[dom].get("bytes_per_beam_chunk"):
-                traffic = tj[dom]["bytes_per_beam_chunk"] * args.beams
+            if dom in tj and tj[dom].get("dram_over_alg"):
+                traffic = round(tj[dom]["dram_over_alg"] * dom_bytes_per_launch)
         except Exception:
             traffic = None
     alg_total = sum(r["alg"])
@@ -368,7 +390,8 @@ def main():
                 "roofline": {"bound": "hbm", "kernel": dom, "launches_per_step": dom_launches_per_step,
                              "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                             "traffic": traffic, "algorithmic_bytes_per_step": dom_bytes},
+                             "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes_per_launch,
+                             "algorithmic_bytes_per_step": dom_bytes},
                 "kernels": {c: {"ms_per_step": round(kt[c][0] / nsteps, 4), "share": round(kt[c][0] / tot_ms, 4) if tot_ms else None,
                                 "alg_GBps": round(r["alg"][i] / (kt[c][0] / nsteps * 1e-3) / 1e9, 1) if kt[c][0] else None}
                             for i, c in enumerate(classes)},
