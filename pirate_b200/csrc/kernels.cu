@@ -37,6 +37,33 @@ template<> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float 
 
 __device__ __forceinline__ float bfly(float x, float y) { return __fmul_rn(kRsqrt2, __fadd_rn(x, y)); }
 
+// Two fp32 additions (multiplications) in one sm_100 packed f32x2 instruction; each element is
+// rounded to nearest like __fadd_rn (__fmul_rn).
+__device__ __forceinline__ unsigned long long f2pack(float2 a)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2unpack(unsigned long long r)
+{
+    float2 d;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(r));
+    return d;
+}
+__device__ __forceinline__ float2 f2add(float2 a, float2 b)
+{
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2pack(a)), "l"(f2pack(b)));
+    return f2unpack(d);
+}
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b)
+{
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2pack(a)), "l"(f2pack(b)));
+    return f2unpack(d);
+}
+
 __device__ __forceinline__ int brev_bits(int x, int nbits) { return nbits ? int(__brev(unsigned(x)) >> (32 - nbits)) : 0; }
 
 static void check_launch(const char *what)
@@ -936,8 +963,56 @@ template<> __device__ __forceinline__ void pf_load4<__nv_bfloat16>(const __nv_bf
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
-template<typename Ts, int L>
-__global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom g)
+// Shared-memory layout of the fast peak finder for one warp (see PfGeom).
+__host__ __device__ constexpr PfGeom pf_geom(int Dout, int Dcore, int tpad, int L, int esize)
+{
+    PfGeom g{};
+    int off = 0;
+    for (int l = 0; l < L; l++) {
+        const int dt = (Dcore < (1 << l)) ? Dcore : (1 << l);
+        const int nsamp = Dout / dt;
+        const bool pairs = ((1 << l) <= Dcore) && nsamp >= 2;
+        const int I = (tpad + dt - (1 << l)) / dt;
+        int k = 0;
+        while ((1 << k) < nsamp) k++;
+        g.off[l] = off;
+        g.e[l] = (nsamp - I % nsamp) % nsamp;
+        g.k[l] = k;
+        // Levels scanned in pairs from per-lane blocks: 2 floats after each block of >= 4 (the
+        // blocks then fall on distinct banks for 8-byte loads); the others are stored contiguously.
+        g.pad[l] = (pairs && nsamp >= 4) ? 2 : 0;
+        g.I[l] = I;
+        g.n[l] = 32 * nsamp + I;
+        g.dt[l] = dt;
+        g.S[l] = (1 << l) / dt;
+        g.nsamp[l] = nsamp;
+        if (l > 0) {
+            const int dtp = (Dcore < (1 << (l - 1))) ? Dcore : (1 << (l - 1));
+            g.rr[l] = dt / dtp;
+            g.ss[l] = (1 << (l - 1)) / dtp;
+        }
+        g.flags[l] = (((1 << l) <= Dcore) ? kPfU : 0) | (pairs ? kPfPairs : 0)
+                   | ((l + 1 < L && (2 << l) <= Dcore) ? kPfNextU : 0);
+        const int t = g.n[l] - 1 + g.e[l];
+        const int size = t + g.pad[l] * (t >> k) + 1;
+        off += (size + 1) & ~1;
+    }
+    g.raw_off = (off + 3) & ~3;
+    const int raw_floats = ((32 * Dout + tpad) * esize + 15) / 16 * 4;
+    g.warp_floats = g.raw_off + raw_floats;
+    return g;
+}
+
+// Peak-finder constants fixed by the plan rules: Dcore = min(Dout, 8) and tpad = max(2 Wmax, 4) with
+// L = max(log2 Wmax, 1), i.e. tpad = max(2^(L+1), 4).
+__host__ __device__ constexpr int pf_dcore_of(int Dout) { return Dout < 8 ? Dout : 8; }
+__host__ __device__ constexpr int pf_tpad_of(int L) { return (2 << L) > 4 ? (2 << L) : 4; }
+
+// The kernel body. g holds the per-level constants (a compile-time constant object when DOUT > 0, so
+// the unrolled level loop sees them as immediates); gr is the same geometry passed at launch, used
+// where the level is only known at run time.
+template<typename Ts, int L, int DOUT>
+__device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, const PfGeom &gr)
 {
     extern __shared__ float sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -952,15 +1027,16 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom
     const bool active = (lane < ntw);
     float *lev = sm + warp * g.warp_floats;
 
-    const int Dout = a.Dout;
+    const int Dout = (DOUT > 0) ? DOUT : a.Dout;
+    const int tpad = (DOUT > 0) ? pf_tpad_of(L) : a.tpad;
     const int Wds = a.ndm_out / a.ndm_wt, Tds = a.nt_out / a.nt_wt;
     const float *wp = a.wt + ((((long) b * a.ndm_wt + dm / Wds) * a.nt_wt + (active ? tout / Tds : 0)) * a.P) * a.N;
     const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
     const int mask = int(a.pf_cap - 1);
     // Window sample 0 (stream time s0 + 32 tile * Dout - tpad, a multiple of 4), as a delay-line slot.
-    const int sbm = int((a.s0 + (long) tout0 * Dout - a.tpad) & (a.pf_cap - 1));
+    const int sbm = int((a.s0 + (long) tout0 * Dout - tpad) & (a.pf_cap - 1));
     const bool full = (L > 1) || (a.P > 1);
-    const int nq0 = (ntw * Dout + a.tpad) >> 2;   // samples the active lanes read (a partial last tile reads fewer)
+    const int nq0 = (ntw * Dout + tpad) >> 2;   // samples the active lanes read (a partial last tile reads fewer)
 
     float best = -1.0e30f;
     int winG = -1;            // group l * M + m of the first maximum; -1: no trial above -1e30
@@ -1031,34 +1107,36 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom
                 float x2 = lev[pf_phys(g, l, j0 - 1)];
                 const float x1 = lev[pf_phys(g, l, j0 - 2)];
                 const float x0 = lev[pf_phys(g, l, j0 - 3)];
-                float hx1 = __fmul_rn(0.5f, x1), hx2 = __fmul_rn(0.5f, x2);
+                float2 H = make_float2(__fmul_rn(0.5f, x1), __fmul_rn(0.5f, x2));   // x[is-2]/2, x[is-1]/2
                 float Ap = __fadd_rn(__fmul_rn(0.5f, x0), x1);
                 const float *xs = lev + pf_phys(g, l, j0);
                 float *ys = lev + (nextU ? pf_phys(g, l + 1, g.I[l + 1] + lane * (nsamp >> 1)) : 0);
+                const float2 W0 = make_float2(w0, w0), W1 = make_float2(w1, w1);
+                const float2 W2 = make_float2(w2, w2), W3 = make_float2(w3, w3);
 
 #pragma unroll 2
                 for (int is = 0; is < nsamp; is += 2) {
-                    const float2 xx = *(const float2 *) (xs + is);
-                    const float xa = xx.x, xb = xx.y;
+                    const float2 X = *(const float2 *) (xs + is);
+                    const float xa = X.x, xb = X.y;
                     float mx;
                     if (full) {
-                        // fine sample is (xa) and is+1 (xb): profiles y1 = x2+x3, y2 = (x1/2+x2)+x3/2,
-                        // y3 = ((x0/2+x1)+x2)+x3/2 with the reference's association.
-                        const float ha = __fmul_rn(0.5f, xa), hb = __fmul_rn(0.5f, xb);
-                        const float Aa = __fadd_rn(hx1, x2), Ab = __fadd_rn(hx2, xa);
-                        const float v1a = __fmul_rn(w1, __fadd_rn(x2, xa));
-                        const float v2a = __fmul_rn(w2, __fadd_rn(Aa, ha));
-                        const float v3a = __fmul_rn(w3, __fadd_rn(__fadd_rn(Ap, x2), ha));
-                        const float v1b = __fmul_rn(w1, __fadd_rn(xa, xb));
-                        const float v2b = __fmul_rn(w2, __fadd_rn(Ab, hb));
-                        const float v3b = __fmul_rn(w3, __fadd_rn(__fadd_rn(Aa, xa), hb));
+                        // Fine samples is (xa) and is+1 (xb), in packed pairs (a, b): profiles
+                        // y1 = x2+x3, y2 = (x1/2+x2)+x3/2, y3 = ((x0/2+x1)+x2)+x3/2 with the reference's
+                        // association; A = x1/2+x2 of each sample, and y3's (x0/2+x1) is the previous A.
+                        const float2 Hn = f2mul(make_float2(0.5f, 0.5f), X);
+                        const float2 Pr = make_float2(x2, xa);       // x[is-1], x[is]
+                        const float2 A = f2add(H, Pr);
+                        const float2 V1 = f2mul(W1, f2add(Pr, X));
+                        const float2 V2 = f2mul(W2, f2add(A, Hn));
+                        const float2 V3 = f2mul(W3, f2add(f2add(make_float2(Ap, A.x), Pr), Hn));
                         if (l == 0) {
-                            const float t = pf_max3(__fmul_rn(w0, xa), v1a, v2a);
-                            mx = fmaxf(pf_max3(t, v3a, __fmul_rn(w0, xb)), pf_max3(v1b, v2b, v3b));
+                            const float2 V0 = f2mul(W0, X);
+                            mx = fmaxf(pf_max3(V0.x, V1.x, V2.x), pf_max3(V3.x, V0.y, V1.y));
+                            mx = pf_max3(mx, V2.y, V3.y);
                         } else {
-                            mx = fmaxf(pf_max3(v1a, v2a, v3a), pf_max3(v1b, v2b, v3b));
+                            mx = fmaxf(pf_max3(V1.x, V2.x, V3.x), pf_max3(V1.y, V2.y, V3.y));
                         }
-                        hx1 = ha; hx2 = hb; x2 = xb; Ap = Ab;
+                        H = Hn; x2 = xb; Ap = A.y;
                     } else {
                         mx = fmaxf(__fmul_rn(w0, xa), __fmul_rn(w0, xb));
                     }
@@ -1122,24 +1200,24 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom
         if (__any_sync(0xffffffffu, upd)) {
             if (upd) {
                 const int l = winL;
-                const int dt = g.dt[l], S = g.S[l], nsamp = g.nsamp[l];
-                const int j0 = g.I[l] + lane * nsamp;
+                const int dt = gr.dt[l], S = gr.S[l], nsamp = gr.nsamp[l];
+                const int j0 = gr.I[l] + lane * nsamp;
                 const float w0 = (l == 0) ? wp[n] : 0.0f;
                 const float w1 = full ? wp[(3 * l + 1) * a.N + n] : 0.0f;
                 const float w2 = full ? wp[(3 * l + 2) * a.N + n] : 0.0f;
                 const float w3 = full ? wp[(3 * l + 3) * a.N + n] : 0.0f;
                 for (int is = winP; is < min(winP + 2, nsamp); is++) {
                     const int j = j0 + is;
-                    const float x3 = lev[pf_phys(g, l, j)];
+                    const float x3 = lev[pf_phys(gr, l, j)];
                     const uint32_t tk0 = (uint32_t(m) << 16) | uint32_t(is * dt);
                     if (l == 0) {
                         const float v0 = __fmul_rn(w0, x3);
                         if (v0 == best) { outv = v0; tok = tk0; break; }
                     }
                     if (full) {
-                        const float x0 = lev[pf_phys(g, l, j - 3 * S)];
-                        const float x1 = lev[pf_phys(g, l, j - 2 * S)];
-                        const float x2 = lev[pf_phys(g, l, j - S)];
+                        const float x0 = lev[pf_phys(gr, l, j - 3 * S)];
+                        const float x1 = lev[pf_phys(gr, l, j - 2 * S)];
+                        const float x2 = lev[pf_phys(gr, l, j - S)];
                         const float hx3 = __fmul_rn(0.5f, x3);
                         const float v1 = __fmul_rn(w1, __fadd_rn(x2, x3));
                         const float v2 = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3));
@@ -1159,6 +1237,19 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom
     const long o = ((long) b * a.ndm_out + dm) * a.nt_out + tout;
     ((Ts *) a.out_max)[o] = from_f<Ts>(outv);
     a.out_argmax[o] = tok;
+}
+
+// DOUT > 0: compiled for that output time downsampling (with Dcore = min(DOUT, 8) and the plan's tpad
+// for L levels); DOUT = 0: any Dout >= 4, geometry read from the launch arguments.
+template<typename Ts, int L, int DOUT>
+__global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom gr)
+{
+    if constexpr (DOUT > 0) {
+        constexpr PfGeom gc = pf_geom(DOUT, pf_dcore_of(DOUT), pf_tpad_of(L), L, sizeof(Ts));
+        pf_fast_body<Ts, L, DOUT>(a, gc, gr);
+    } else {
+        pf_fast_body<Ts, L, 0>(a, gr, gr);
+    }
 }
 
 
@@ -1271,45 +1362,6 @@ int pf_warp_floats(int Dout, int tpad, int Dcore, int L)
     return tot;
 }
 
-// Shared-memory layout of the fast peak finder for one warp (see PfGeom).
-static PfGeom pf_geom(int Dout, int Dcore, int tpad, int L, int esize)
-{
-    PfGeom g{};
-    int off = 0;
-    for (int l = 0; l < L; l++) {
-        const int dt = (Dcore < (1 << l)) ? Dcore : (1 << l);
-        const int nsamp = Dout / dt;
-        const bool pairs = ((1 << l) <= Dcore) && nsamp >= 2;
-        const int I = (tpad + dt - (1 << l)) / dt;
-        int k = 0;
-        while ((1 << k) < nsamp) k++;
-        g.off[l] = off;
-        g.e[l] = (nsamp - I % nsamp) % nsamp;
-        g.k[l] = k;
-        // Levels scanned in pairs from per-lane blocks: 2 floats after each block of >= 4 (the
-        // blocks then fall on distinct banks for 8-byte loads); the others are stored contiguously.
-        g.pad[l] = (pairs && nsamp >= 4) ? 2 : 0;
-        g.I[l] = I;
-        g.n[l] = 32 * nsamp + I;
-        g.dt[l] = dt;
-        g.S[l] = (1 << l) / dt;
-        g.nsamp[l] = nsamp;
-        if (l > 0) {
-            const int dtp = (Dcore < (1 << (l - 1))) ? Dcore : (1 << (l - 1));
-            g.rr[l] = dt / dtp;
-            g.ss[l] = (1 << (l - 1)) / dtp;
-        }
-        g.flags[l] = (((1 << l) <= Dcore) ? kPfU : 0) | (pairs ? kPfPairs : 0)
-                   | ((l + 1 < L && (2 << l) <= Dcore) ? kPfNextU : 0);
-        const int t = g.n[l] - 1 + g.e[l];
-        const int size = t + g.pad[l] * (t >> k) + 1;
-        off += (size + 1) & ~1;
-    }
-    g.raw_off = (off + 3) & ~3;
-    const int raw_floats = ((32 * Dout + tpad) * esize + 15) / 16 * 4;
-    g.warp_floats = g.raw_off + raw_floats;
-    return g;
-}
 
 // The fast kernel needs 4-sample runs of the window (Dout >= 4, tpad and s0 multiples of 4).
 static bool pf_fast_ok(const PfArgs &a)
@@ -1317,16 +1369,27 @@ static bool pf_fast_ok(const PfArgs &a)
     return a.Dout >= 4 && (a.tpad % 4) == 0 && (a.s0 % 4) == 0 && (a.pf_cap % 4) == 0 && a.L <= 5;
 }
 
+template<typename Ts, int L, int DOUT>
+static void launch_pf_fast(const PfArgs &a, const PfGeom &g, int B, cudaStream_t s)
+{
+    size_t sm = (size_t) kPfWarps * g.warp_floats * sizeof(float);
+    set_smem(pf_fast_kernel<Ts, L, DOUT>, sm);
+    dim3 grid((a.nt_out + 31) / 32, (a.ndm_out + kPfWarps - 1) / kPfWarps, B);
+    pf_fast_kernel<Ts, L, DOUT><<<grid, kPfWarps * 32, sm, s>>>(a, g);
+    check_launch("pf_fast_kernel");
+}
+
 template<typename Ts, int L>
 static void launch_pf_l(const PfArgs &a, int B, cudaStream_t s)
 {
     if (pf_fast_ok(a)) {
         const PfGeom g = pf_geom(a.Dout, a.Dcore, a.tpad, L, (int) sizeof(Ts));
-        size_t sm = (size_t) kPfWarps * g.warp_floats * sizeof(float);
-        set_smem(pf_fast_kernel<Ts, L>, sm);
-        dim3 grid((a.nt_out + 31) / 32, (a.ndm_out + kPfWarps - 1) / kPfWarps, B);
-        pf_fast_kernel<Ts, L><<<grid, kPfWarps * 32, sm, s>>>(a, g);
-        check_launch("pf_fast_kernel");
+        // Compiled geometries for the usual output downsamplings (pirate's default Dout = 2^pf_rank).
+        const bool std_geom = (a.Dcore == pf_dcore_of(a.Dout)) && (a.tpad == pf_tpad_of(L));
+        if (std_geom && a.Dout == 16) launch_pf_fast<Ts, L, 16>(a, g, B, s);
+        else if (std_geom && a.Dout == 8) launch_pf_fast<Ts, L, 8>(a, g, B, s);
+        else if (std_geom && a.Dout == 4) launch_pf_fast<Ts, L, 4>(a, g, B, s);
+        else launch_pf_fast<Ts, L, 0>(a, g, B, s);
         return;
     }
     int wf = pf_warp_floats(a.Dout, a.tpad, a.Dcore, a.L);
