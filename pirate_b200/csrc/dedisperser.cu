@@ -251,6 +251,12 @@ void GpuDedisperser::allocate()
                 tot += cap[row];
             }
             st.ring_beam_stride = tot;
+            // The stage-1 kernel indexes a block's 2^R1 delay lines with 32-bit offsets.
+            for (long blk = 0; blk < st.nblocks; blk++) {
+                long end = (blk + 1 < st.nblocks) ? off[(blk + 1) * pow2(R1)] : tot;
+                if (end - off[blk * pow2(R1)] >= (1L << 31))
+                    throw runtime_error("GpuDedisperser::allocate(): stage-1 delay lines of one block exceed 2^31 samples");
+            }
             st.ring_off.upload(off.data(), off.size() * sizeof(long));
             st.ring_cap.upload(cap.data(), cap.size() * sizeof(int));
             add(st.ring, size_t(total_beams) * tot * esize);

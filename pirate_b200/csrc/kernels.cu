@@ -254,9 +254,11 @@ __device__ __forceinline__ void bfly_l0_shared(float &v0, float &v1, float *h, i
 
 // All K steps of a register tree, in place. pv[r][q] holds pair q's row0 input of the previous tile.
 // With HS, the lag-0 pairs keep that history in shared memory (hs[slot], one float per pair, in
-// (r, q) order), which frees their registers.
-template<int K, bool HS = false>
-__device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>::NS][RT<K>::NP], int lane, float *hs = nullptr)
+// (r, q) order), which frees their registers. With EXT0, step 0 (all lags 0) takes its lag-1
+// operands from b0[q] = row 2q one sample earlier, supplied by the caller, and keeps no history.
+template<int K, bool HS = false, bool EXT0 = false>
+__device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>::NS][RT<K>::NP], int lane, float *hs = nullptr,
+                                         const float *b0 = nullptr)
 {
     int slot = 0;
 #pragma unroll
@@ -266,6 +268,12 @@ __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>
             const int h = 1 << r;
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
             const int L = rt_lag(r, q);
+            if (EXT0 && r == 0) {
+                const float x = v[i0], y = v[i0 + 1];
+                v[i0] = bfly(x, y);
+                v[i0 + 1] = bfly(b0[q], y);
+                continue;
+            }
             if (HS && L == 0) {
                 bfly_l0_shared(v[i0], v[i0 + h], hs + slot, lane);
                 slot++;
@@ -283,7 +291,7 @@ __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>
 
 // Persistent histories: pair (r, q) needs its previous-tile row0 only in lanes >= 31 - lag.
 // With HS the lag-0 pairs' single value goes to or comes from hs[slot].
-template<int K, bool HS = false>
+template<int K, bool HS = false, bool EXT0 = false>
 __device__ __forceinline__ void rt_load(float (&pv)[RT<K>::NS][RT<K>::NP], const float *st, int lane, float *hs = nullptr)
 {
     int off = 0, slot = 0;
@@ -292,7 +300,9 @@ __device__ __forceinline__ void rt_load(float (&pv)[RT<K>::NS][RT<K>::NP], const
 #pragma unroll
         for (int q = 0; q < RT<K>::NP; q++) {
             const int L = rt_lag(r, q);
-            if (HS && L == 0) {
+            if (EXT0 && r == 0) {
+                // no history (its state slot stays unused)
+            } else if (HS && L == 0) {
                 if (lane == 0) hs[slot] = st[off];
                 slot++;
             } else {
@@ -304,7 +314,7 @@ __device__ __forceinline__ void rt_load(float (&pv)[RT<K>::NS][RT<K>::NP], const
     if (HS) __syncwarp();
 }
 
-template<int K, bool HS = false>
+template<int K, bool HS = false, bool EXT0 = false>
 __device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP], float *st, int lane, const float *hs = nullptr)
 {
     if (HS) __syncwarp();
@@ -314,7 +324,8 @@ __device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP],
 #pragma unroll
         for (int q = 0; q < RT<K>::NP; q++) {
             const int L = rt_lag(r, q);
-            if (HS && L == 0) {
+            if (EXT0 && r == 0) {
+            } else if (HS && L == 0) {
                 if (lane == 0) st[off] = hs[slot];
                 slot++;
             } else {
@@ -329,10 +340,10 @@ __device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP],
 // pf level r'+1 are emitted (FrequencySubbands multiplet order), reproducing ReferenceTree::dedisperse_2d
 // (src_lib/ReferenceTree.cpp:120-300): even band pairs coincide with the in-place butterflies, odd
 // ("staggered") pairs (2k+1, 2k+2) are extra butterflies with their own histories ps[r'][u].
-template<int RB, bool STAG, bool HS, typename Emit>
+template<int RB, bool STAG, bool HS, bool EXT0, typename Emit>
 __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv)[RT<RB>::NS][RT<RB>::NP],
                                                  float (&ps)[RT<RB>::NS][RT<RB>::NP], const Stage2Args &a,
-                                                 int lane, Emit emit, float *hs)
+                                                 int lane, Emit emit, float *hs, const float *b0)
 {
     constexpr int NB = 1 << RB;
     int slot = 0;   // HS: lag-0 in-place pairs keep their history in hs[slot] (see rt_steps)
@@ -364,7 +375,11 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
             const int k = q >> r, j = q & (h - 1);
             const int L = rt_lag(r, q);
-            if (HS && L == 0) {
+            if (EXT0 && r == 0) {
+                const float x = v[i0], y = v[i0 + 1];
+                v[i0] = bfly(x, y);
+                v[i0 + 1] = bfly(b0[q], y);
+            } else if (HS && L == 0) {
                 bfly_l0_shared(v[i0], v[i0 + h], hs + slot, lane);
                 slot++;
             } else {
@@ -436,17 +451,43 @@ struct PfEmit
 // off(rr) and has capacity cap(rr) = ring_cap(f, d), a multiple of 32. Phase a writes tile k at
 // wpos, phase b reads tile k-1 at rpos - P(f, d); positions are multiples of 32, so a write never
 // wraps and a read wraps at most once. Per row the tables hold
-//   wb[rr] = off + wpos                          (phase a: write index of lane 0)
-//   rt[rr] = {off + rpos - P, off, cap, off + cap - P}   (phase b: read index of lane 0, wrap bounds)
+//   wb[f * 2^RA + d] = off + wpos                 (phase a: write index of lane 0)
+//   rt[d * 2^RB + f] = {off + rpos - P, off | cap << 16}   (phase b: read index of lane 0, wrap bounds)
+// so that each warp's rows are consecutive (128-bit table loads).
 template<int RA, int RB>
 __device__ __forceinline__ int ring_lag(int f, int d) { return ((1 << RB) - 1 - f) * brev_bits(d, RA); }
 
 __device__ __forceinline__ int wrap_add(int p, int cap) { return (p >= cap) ? (p - cap) : ((p < 0) ? (p + cap) : p); }
 
+// Entry i of a warp's consecutive table row (16-byte aligned base; four ints or two int2 per 128-bit
+// shared load, the fields selected at compile time in the unrolled loops that call these).
+// N = entries per row: 128-bit loads need N a multiple of 4 (int) or 2 (int2), which keeps every
+// row base 16-byte aligned; smaller rows use plain loads.
+template<int N>
+__device__ __forceinline__ int tab_int(const int *base, int i)
+{
+    if constexpr (N % 4 != 0) {
+        return base[i];
+    } else {
+        const int4 t = ((const int4 *) base)[i >> 2];
+        return ((i & 3) == 0) ? t.x : ((i & 3) == 1) ? t.y : ((i & 3) == 2) ? t.z : t.w;
+    }
+}
+template<int N>
+__device__ __forceinline__ int2 tab_int2(const int2 *base, int i)
+{
+    if constexpr (N % 2 != 0) {
+        return base[i];
+    } else {
+        const int4 t = ((const int4 *) base)[i >> 1];
+        return (i & 1) ? make_int2(t.z, t.w) : make_int2(t.x, t.y);
+    }
+}
+
 // Fills wb[] and rt[] for stream time s0 (a multiple of 32). Uses ioff[NR] as scratch; ends with
 // __syncthreads().
 template<int RA, int RB>
-__device__ void ring_init(int *wb, int4 *rt, int *ioff, long s0)
+__device__ void ring_init(int *wb, int2 *rt, int *ioff, long s0)
 {
     constexpr int NR = 1 << (RA + RB);
     const int rr = threadIdx.x;
@@ -467,7 +508,7 @@ __device__ void ring_init(int *wb, int4 *rt, int *ioff, long s0)
         const int off = ioff[rr], cap = ring_cap(RA, RB, f, d), P = ring_lag<RA, RB>(f, d);
         const int pos = int(s0 % cap);
         wb[rr] = off + pos;
-        rt[rr] = make_int4(off + pos - P, off, cap, off + cap - P);
+        rt[d * (1 << RB) + f] = make_int2(off + pos - P, off | (cap << 16));
     }
     __syncthreads();
 }
@@ -498,11 +539,12 @@ template<typename Ts, int RA, int RB>
 struct TreeSmem
 {
     static constexpr int NR = 1 << (RA + RB);
+    static_assert(NR >= 2 && ring_floats(RA, RB) < 65536, "delay-line tables pack offset and capacity in 16 bits");
     static constexpr size_t in_off = 0;                       // long[NR]
-    static constexpr size_t out_base = in_off + 8 * NR;       // long[NR]
-    static constexpr size_t out_off = out_base + 8 * NR;      // long[NR]
-    static constexpr size_t rt = out_off + 8 * NR;            // int4[NR]
-    static constexpr size_t wb = rt + 16 * NR;                // int[NR]
+    static constexpr size_t out_base = in_off + 8 * NR;       // int[NR]
+    static constexpr size_t out_off = out_base + 4 * NR;      // int[NR]
+    static constexpr size_t rt = out_off + 4 * NR;            // int2[NR]
+    static constexpr size_t wb = rt + 8 * NR;                 // int[NR]
     static constexpr size_t in_pos = wb + 4 * NR;             // int[NR]
     static constexpr size_t in_cap = in_pos + 4 * NR;         // int[NR]
     static constexpr size_t hist = in_cap + 4 * NR;           // float[warps][16]: lag-0 histories
@@ -535,9 +577,11 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     extern __shared__ __align__(16) unsigned char sm_raw[];
 
     long *in_off = (long *) (sm_raw + Lay::in_off);       // stage 2: input delay line offsets
-    long *out_base = (long *) (sm_raw + Lay::out_base);   // stage 1: output delay line index of lane 0
-    long *out_off = (long *) (sm_raw + Lay::out_off);     // stage 1: output delay line offsets
-    int4 *rt = (int4 *) (sm_raw + Lay::rt);
+    // stage 1, per output row (f, d) at [d * NB + f]: index of lane 0 and start of its delay line,
+    // relative to the block's first line
+    int *out_base = (int *) (sm_raw + Lay::out_base);
+    int *out_off = (int *) (sm_raw + Lay::out_off);
+    int2 *rt = (int2 *) (sm_raw + Lay::rt);
     int *wb = (int *) (sm_raw + Lay::wb);
     int *in_pos = (int *) (sm_raw + Lay::in_pos);         // stage 2: input read positions
     int *in_cap = (int *) (sm_raw + Lay::in_cap);         // stage 2: input capacities; stage 1: output capacities
@@ -546,6 +590,9 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *hs = (float *) (sm_raw + Lay::hist) + warp * 16;   // this warp's lag-0 histories (HS)
+    // Phase-b step 0 reads its lag-1 operands from the shared delay line (stage 1; in stage 2 the
+    // extra live values cost more in register spills than the shuffles they save).
+    constexpr bool E0 = (STAGE == 1);
     const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
     float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
 
@@ -558,12 +605,14 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     if constexpr (STAGE == 1) {
         in = (const Ts *) a.in + (long) (a.in_beam0 + b) * a.in_beam_stride + (long) blk * NR * a.in_row_stride;
         pos1 = int(a.in_s0 & a.in_mask);
+        const long off0 = a.ring_off[(long) blk * NR];   // the host checks that a block's lines span < 2^31
         for (int r = threadIdx.x; r < NR; r += blockDim.x) {
             const int cap = a.ring_cap[(long) blk * NR + r];   // capacity of output delay line r (a multiple of 32)
-            const long off = a.ring_off[(long) blk * NR + r];
-            in_cap[r] = cap;
-            out_off[r] = off;
-            out_base[r] = off + a.s0 % cap;
+            const int off = int(a.ring_off[(long) blk * NR + r] - off0);
+            const int j = (r & (NA - 1)) * NB + (r >> RA);      // row (f, d) = r at [d * NB + f]
+            in_cap[j] = cap;
+            out_off[j] = off;
+            out_base[j] = off + int(a.s0 % cap);
         }
     } else {
         in = (const Ts *) a.ring + (long) bt * a.ring_beam_stride;
@@ -651,11 +700,12 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 rt_steps<RA, HS>(v, pva, lane, hs);
 #pragma unroll
                 for (int i = 0; i < NA; i++)
-                    ring[wb[g * NA + i] + lane] = v[i];
+                    ring[tab_int<NA>(wb + g * NA, i) + lane] = v[i];
                 __syncwarp();
                 if (lane < NA) {
                     const int rr = g * NA + lane;
-                    const int lo = rt[rr].y, cap = rt[rr].z;   // phase b updates only rt[].x
+                    const int y = rt[lane * NB + g].y;   // phase b updates only rt[].x
+                    const int lo = y & 0xffff, cap = y >> 16;
                     const int w = wb[rr] + 32;
                     wb[rr] = (w == lo + cap) ? lo : w;
                 }
@@ -667,7 +717,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     } else {
         float pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
         float *stb = st + RING + NB * rt_state(RA) + g * (rt_state(RB) + (STAGE == 2 ? st_state(RB) : 0));
-        rt_load<RB, HS>(pvb, stb, lane, hs);
+        rt_load<RB, HS, E0>(pvb, stb, lane, hs);
         if (STAG) st_load<RB>(psb, stb + rt_state(RB), lane);
 
         PfEmit<Ts> emit;
@@ -683,42 +733,50 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
 
         for (int it = 0; it <= ntiles; it++) {
             if (it >= 1) {
-                float v[NB];
+                // Phase-b rows, and (E0) for step 0 (lag 0) each even row one sample earlier: the delay
+                // line holds it (capacity >= P + 65), so no shuffle and no history are needed.
+                float v[NB], b0[RT<RB>::NP];
 #pragma unroll
                 for (int f = 0; f < NB; f++) {
-                    const int4 t = rt[f * NA + g];
+                    const int2 t = tab_int2<NB>(rt + g * NB, f);
+                    const int lo = t.y & 0xffff, cap = t.y >> 16;
                     int q = t.x + lane;
-                    q = (q < t.y) ? (q + t.z) : q;
+                    q = (q < lo) ? (q + cap) : q;
                     v[f] = ring[q];
+                    if (E0 && (f & 1) == 0 && RB > 0) {
+                        const int qm = (q == lo) ? (q + cap - 1) : (q - 1);
+                        b0[f >> 1] = ring[qm];
+                    }
                 }
                 __syncwarp();
                 if (lane < NB) {
-                    const int rr = lane * NA + g;
-                    const int4 t = rt[rr];
+                    const int rr = g * NB + lane;   // row (f = lane, d = g)
+                    const int2 t = rt[rr];
+                    const int lo = t.y & 0xffff, cap = t.y >> 16;
                     const int x = t.x + 32;
-                    rt[rr].x = (x >= t.w) ? (x - t.z) : x;
+                    rt[rr].x = (x >= lo + cap - ring_lag<RA, RB>(lane, g)) ? (x - cap) : x;
                 }
                 if constexpr (STAGE == 1) {
-                    rt_steps<RB, HS>(v, pvb, lane, hs);
-                    Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride;
+                    rt_steps<RB, HS, E0>(v, pvb, lane, hs, b0);
+                    Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride + a.ring_off[(long) blk * NR];
 #pragma unroll
                     for (int f = 0; f < NB; f++)
-                        out[out_base[(f << RA) | g] + lane] = from_f<Ts>(v[f]);
+                        out[tab_int<NB>(out_base + g * NB, f) + lane] = from_f<Ts>(v[f]);
                     __syncwarp();
                     if (lane < NB) {
-                        const int i = (lane << RA) | g;
-                        const long ob = out_base[i] + 32;
+                        const int i = g * NB + lane;
+                        const int ob = out_base[i] + 32;
                         out_base[i] = (ob == out_off[i] + in_cap[i]) ? out_off[i] : ob;
                     }
                 } else {
                     emit.row0 = pf_rows + pf_slot;
                     pf_slot = (pf_slot + 32) & int(a.pf_cap - 1);
-                    phase_b_subbands<RB, STAG, HS>(v, pvb, psb, a, lane, emit, hs);
+                    phase_b_subbands<RB, STAG, HS, E0>(v, pvb, psb, a, lane, emit, hs, b0);
                 }
             }
             asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
         }
-        rt_save<RB, HS>(pvb, stb, lane, hs);
+        rt_save<RB, HS, E0>(pvb, stb, lane, hs);
         if (STAG) st_save<RB>(psb, stb + rt_state(RB), lane);
     }
     __syncthreads();

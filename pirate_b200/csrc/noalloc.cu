@@ -129,6 +129,11 @@ void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, cons
             tot += cap[row];
         }
         st.ring_stride = tot;
+        for (long blk = 0; blk < st.nblocks; blk++) {   // 32-bit offsets within a block's delay lines
+            long end = (blk + 1 < st.nblocks) ? off[(blk + 1) * (1L << R1)] : tot;
+            if (end - off[blk * (1L << R1)] >= (1L << 31))
+                throw std::runtime_error("pb2_dedisperse_chunk_noalloc: stage-1 delay lines of one block exceed 2^31 samples");
+        }
         st.ring_off_t = tab.put(off.data(), nrows * sizeof(long));
         st.ring_cap_t = tab.put(cap.data(), nrows * sizeof(int));
         st.state_pb = stage1_state_floats(R1);

@@ -76,11 +76,12 @@ __host__ __device__ constexpr int st_off(int K, int r0, int u0)
     return s;
 }
 
-// Delay line between the phases: row (f, d) holds P(f, d) + 64 samples (phase a writes tile k while
-// phase b reads tile k-1), rounded up to a multiple of 32 so that a tile never wraps on write.
+// Delay line between the phases: row (f, d) holds P(f, d) + 65 samples (phase a writes tile k while
+// phase b reads tile k-1 and, for step 0, the sample before it), rounded up to a multiple of 32 so
+// that a tile never wraps on write.
 __host__ __device__ constexpr int ring_cap(int RA, int RB, int f, int d)
 {
-    return (((1 << RB) - 1 - f) * bitrev_c(d, RA) + 64 + 31) & ~31;
+    return (((1 << RB) - 1 - f) * bitrev_c(d, RA) + 65 + 31) & ~31;
 }
 
 __host__ __device__ constexpr int ring_floats(int RA, int RB)
