@@ -148,41 +148,47 @@ __device__ __forceinline__ void grid_run(const GridLdsArgs &a, const Ts *xb, lon
     }
 }
 
+constexpr int kGridMaxThreads = 512;
+
 template<typename Ts, int NLEV>
-__global__ void __launch_bounds__(128) grid_lds_kernel(GridLdsArgs a)
+__global__ void __launch_bounds__(kGridMaxThreads) grid_lds_kernel(GridLdsArgs a)
 {
     constexpr int W0 = ((1 << NLEV) > 8) ? (1 << NLEV) : 8;
     constexpr int WE = 1 << NLEV;           // level-0 samples feeding one level-NLEV sample
+    __shared__ float xch[(NLEV > 0) ? NLEV : 1][kGridMaxThreads];
 
     const long nhalf = 1L << (a.rank - 1);
     const long nwin = a.T / W0;
     const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= nwin * nhalf * a.B)
-        return;
-    const int win = int(g % nwin);
-    const long c = (g / nwin) % nhalf;
-    const int b = int(g / (nwin * nhalf));
+    // Threads past the end take part in the block barrier only.
+    const bool live = g < nwin * nhalf * a.B;
+    const long gg = live ? g : 0;
+    const int win = int(gg % nwin);
+    const long c = (gg / nwin) % nhalf;
+    const int b = int(gg / (nwin * nhalf));
     const int bt = a.beam0 + b;
     const int parity = int(a.ichunk & 1);
     const long t0 = (long) win * W0;
 
     const Ts *xb = (const Ts *) a.in + (long) b * a.F * a.T;
     float r0[W0], r1[W0];
-    grid_run<Ts, W0>(a, xb, 2 * c, t0, r0);
-    grid_run<Ts, W0>(a, xb, 2 * c + 1, t0, r1);
-    Ts *lev0 = (Ts *) a.tree0 + ((long) b * (2 * nhalf) + 2 * c) * a.T + t0;
-    store_run<Ts, W0>(lev0, r0);
-    store_run<Ts, W0>(lev0 + a.T, r1);
+    if (live) {
+        grid_run<Ts, W0>(a, xb, 2 * c, t0, r0);
+        grid_run<Ts, W0>(a, xb, 2 * c + 1, t0, r1);
+        Ts *lev0 = (Ts *) a.tree0 + ((long) b * (2 * nhalf) + 2 * c) * a.T + t0;
+        store_run<Ts, W0>(lev0, r0);
+        store_run<Ts, W0>(lev0 + a.T, r1);
+    }
 
     if constexpr (NLEV > 0) {
-        float e[WE];
-        if (win > 0)
-            grid_run<Ts, WE>(a, xb, 2 * c, t0 - WE, e);
-
+        // Level p of each channel: in place, r[u] = (r[2u] + r[2u+1]) / sqrt2. The odd channel's output
+        // sample u pairs with the even channel's sample u-1; for u = 0 that is the last sample of the
+        // previous window at this level (the thread before, exchanged through shared memory), or at
+        // the chunk start the saved state.
+        float first[NLEV], last[NLEV];
 #pragma unroll
         for (int p = 1; p <= NLEV; p++) {
             const int len = W0 >> p;
-            const int elen = WE >> p;
 #pragma unroll
             for (int u = 0; u < (W0 >> 1); u++) {
                 if (u < len) {
@@ -190,29 +196,55 @@ __global__ void __launch_bounds__(128) grid_lds_kernel(GridLdsArgs a)
                     r1[u] = bfly(r1[2 * u], r1[2 * u + 1]);
                 }
             }
-            float prev;
-            if (win > 0) {
-#pragma unroll
-                for (int u = 0; u < (WE >> 1); u++)
-                    if (u < elen) e[u] = bfly(e[2 * u], e[2 * u + 1]);
-                prev = e[elen - 1];
-            } else {
-                prev = a.state[(((long) parity * a.total_beams + bt) * a.nlev + (p - 1)) * nhalf + c];
-            }
+            first[p - 1] = r1[0];
+            last[p - 1] = r0[len - 1];
+            xch[p - 1][threadIdx.x] = r0[len - 1];
 
-            const long cap = a.cap_mask[p - 1] + 1;
-            Ts *ring = (Ts *) a.ring[p - 1] + ((long) bt * nhalf + c) * cap;
-            const long nt_p = a.T >> p;
-            const long s_base = a.ichunk * nt_p + (long) win * len + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
+            if (live) {
+                const long cap = a.cap_mask[p - 1] + 1;
+                Ts *ring = (Ts *) a.ring[p - 1] + ((long) bt * nhalf + c) * cap;
+                const long nt_p = a.T >> p;
+                const long s_base = a.ichunk * nt_p + (long) win * len + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
 #pragma unroll
-            for (int u = 0; u < (W0 >> 1); u++) {
-                if (u < len) {
-                    float lagged = (u == 0) ? prev : r0[u - 1];
-                    ring[(s_base + u) & a.cap_mask[p - 1]] = from_f<Ts>(bfly(lagged, r1[u]));
+                for (int u = 1; u < (W0 >> 1); u++)
+                    if (u < len)
+                        ring[(s_base + u) & a.cap_mask[p - 1]] = from_f<Ts>(bfly(r0[u - 1], r1[u]));
+                if (win == nwin - 1)
+                    a.state[(((long) (1 - parity) * a.total_beams + bt) * a.nlev + (p - 1)) * nhalf + c] = last[p - 1];
+            }
+        }
+        __syncthreads();
+
+        if (live) {
+            float prev[NLEV];
+            if (win == 0) {
+#pragma unroll
+                for (int p = 1; p <= NLEV; p++)
+                    prev[p - 1] = a.state[(((long) parity * a.total_beams + bt) * a.nlev + (p - 1)) * nhalf + c];
+            } else if (threadIdx.x > 0) {
+#pragma unroll
+                for (int p = 1; p <= NLEV; p++)
+                    prev[p - 1] = xch[p - 1][threadIdx.x - 1];
+            } else {
+                // The previous window belongs to the previous block: grid its WE samples again.
+                float e[WE];
+                grid_run<Ts, WE>(a, xb, 2 * c, t0 - WE, e);
+#pragma unroll
+                for (int p = 1; p <= NLEV; p++) {
+#pragma unroll
+                    for (int u = 0; u < (WE >> 1); u++)
+                        if (u < (WE >> p)) e[u] = bfly(e[2 * u], e[2 * u + 1]);
+                    prev[p - 1] = e[(WE >> p) - 1];
                 }
             }
-            if (win == nwin - 1)
-                a.state[(((long) (1 - parity) * a.total_beams + bt) * a.nlev + (p - 1)) * nhalf + c] = r0[len - 1];
+#pragma unroll
+            for (int p = 1; p <= NLEV; p++) {
+                const long cap = a.cap_mask[p - 1] + 1;
+                Ts *ring = (Ts *) a.ring[p - 1] + ((long) bt * nhalf + c) * cap;
+                const long nt_p = a.T >> p;
+                const long s_base = a.ichunk * nt_p + (long) win * (W0 >> p) + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
+                ring[s_base & a.cap_mask[p - 1]] = from_f<Ts>(bfly(prev[p - 1], first[p - 1]));
+            }
         }
     }
 }
@@ -540,13 +572,12 @@ struct TreeSmem
 {
     static constexpr int NR = 1 << (RA + RB);
     static_assert(NR >= 2 && ring_floats(RA, RB) < 65536, "delay-line tables pack offset and capacity in 16 bits");
-    static constexpr size_t in_off = 0;                       // long[NR]
-    static constexpr size_t out_base = in_off + 8 * NR;       // int[NR]
+    static constexpr size_t in_tab = 0;                       // int4[NR]
+    static constexpr size_t out_base = in_tab + 16 * NR;      // int[NR]
     static constexpr size_t out_off = out_base + 4 * NR;      // int[NR]
     static constexpr size_t rt = out_off + 4 * NR;            // int2[NR]
     static constexpr size_t wb = rt + 8 * NR;                 // int[NR]
-    static constexpr size_t in_pos = wb + 4 * NR;             // int[NR]
-    static constexpr size_t in_cap = in_pos + 4 * NR;         // int[NR]
+    static constexpr size_t in_cap = wb + 4 * NR;             // int[NR]
     static constexpr size_t hist = in_cap + 4 * NR;           // float[warps][16]: lag-0 histories
     static constexpr size_t staging = (hist + 4 * 16 * ((1 << RA) + (1 << RB)) + 15) & ~size_t(15);
     static constexpr size_t ring = (staging + 2 * (1 << RB) * (1 << RA) * Stage<Ts>::SPR * sizeof(Ts) + 15) & ~size_t(15);
@@ -576,15 +607,15 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     using Lay = TreeSmem<Ts, RA, RB>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
 
-    long *in_off = (long *) (sm_raw + Lay::in_off);       // stage 2: input delay line offsets
+    // stage 2, per input row: {read position, capacity, offset low and high words} of its delay line
+    int4 *in_tab = (int4 *) (sm_raw + Lay::in_tab);
     // stage 1, per output row (f, d) at [d * NB + f]: index of lane 0 and start of its delay line,
     // relative to the block's first line
     int *out_base = (int *) (sm_raw + Lay::out_base);
     int *out_off = (int *) (sm_raw + Lay::out_off);
     int2 *rt = (int2 *) (sm_raw + Lay::rt);
     int *wb = (int *) (sm_raw + Lay::wb);
-    int *in_pos = (int *) (sm_raw + Lay::in_pos);         // stage 2: input read positions
-    int *in_cap = (int *) (sm_raw + Lay::in_cap);         // stage 2: input capacities; stage 1: output capacities
+    int *in_cap = (int *) (sm_raw + Lay::in_cap);         // stage 1: output delay line capacities
     Ts *staging = (Ts *) (sm_raw + Lay::staging);
     float *ring = (float *) (sm_raw + Lay::ring);
 
@@ -622,9 +653,8 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
             long lag = (long) (NR - 1 - r) * dm1;
             long cap = a.ring_cap[row];
             long p = (a.s0 - lag) % cap;
-            in_pos[r] = int(p < 0 ? p + cap : p);
-            in_cap[r] = int(cap);
-            in_off[r] = a.ring_off[row];
+            const long off = a.ring_off[row];
+            in_tab[r] = make_int4(int(p < 0 ? p + cap : p), int(cap), int(off & 0xffffffffL), int(off >> 32));
         }
     }
 
@@ -660,15 +690,16 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 constexpr int EPC = Stage<Ts>::EPC, CPR = 32 / EPC + 1;
                 for (int c = lane; c < NA * CPR; c += 32) {
                     const int i = c / CPR, k = c - i * CPR, r = g * NA + i;
-                    const int cap = in_cap[r];
-                    int q = (in_pos[r] & ~(EPC - 1)) + k * EPC;
+                    const int4 t = in_tab[r];
+                    const int cap = t.y;
+                    int q = (t.x & ~(EPC - 1)) + k * EPC;
                     q = (q >= cap) ? (q - cap) : q;
-                    cp_async_bytes<16>(dst + i * SPRK + k * EPC, in + in_off[r] + q);
+                    cp_async_bytes<16>(dst + i * SPRK + k * EPC, in + ((long) t.w << 32 | (unsigned) t.z) + q);
                 }
                 __syncwarp();
                 if (lane < NA) {
                     const int rr = g * NA + lane;
-                    in_pos[rr] = wrap_add(in_pos[rr] + 32, in_cap[rr]);
+                    in_tab[rr].x = wrap_add(in_tab[rr].x + 32, in_tab[rr].y);
                 }
             }
             __syncwarp();
@@ -681,7 +712,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
         if (STAGE == 2) {
 #pragma unroll
             for (int i = 0; i < NA; i++)
-                offs |= (unsigned long long) (in_pos[g * NA + i] & (Stage<Ts>::EPC - 1)) << (OB * i);
+                offs |= (unsigned long long) (in_tab[g * NA + i].x & (Stage<Ts>::EPC - 1)) << (OB * i);
         }
         issue(0);
         cp_async_commit();
@@ -1320,8 +1351,12 @@ static void launch_grid_lds_t(const GridLdsArgs &a, cudaStream_t s)
 {
     constexpr int W0 = ((1 << NLEV) > 8) ? (1 << NLEV) : 8;
     if (a.T % W0) throw std::runtime_error("grid_lds_kernel: chunk length not a multiple of the window");
-    long nthr = (long) (a.T / W0) * (1L << (a.rank - 1)) * a.B;
-    grid_lds_kernel<Ts, NLEV><<<(unsigned) ((nthr + 127) / 128), 128, 0, s>>>(a);
+    const long nwin = a.T / W0;
+    long nthr = nwin * (1L << (a.rank - 1)) * a.B;
+    // Blocks start at a window 0 (a multiple of nwin threads, about 128), so that every other window's
+    // predecessor is computed in the same block.
+    int bd = (nwin <= 128) ? int(nwin * (128 / nwin)) : (nwin <= kGridMaxThreads ? int(nwin) : kGridMaxThreads);
+    grid_lds_kernel<Ts, NLEV><<<(unsigned) ((nthr + bd - 1) / bd), bd, 0, s>>>(a);
     check_launch("grid_lds_kernel");
 }
 
