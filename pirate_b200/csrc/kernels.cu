@@ -379,33 +379,37 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
 {
     constexpr int NB = 1 << RB;
     int slot = 0;   // HS: lag-0 in-place pairs keep their history in hs[slot] (see rt_steps)
+    // Band counts are the same for every tile: each level's emission is skipped as a whole when empty.
+    if (a.sb_count[0] > 0) {
 #pragma unroll
-    for (int f = 0; f < NB; f++)
-        if (f < a.sb_count[0]) emit(a.sb_mbase[0] + f, v[f]);
+        for (int f = 0; f < NB; f++)
+            if (f < a.sb_count[0]) emit(a.sb_mbase[0] + f, v[f]);
+    }
 
 #pragma unroll
     for (int r = 0; r < RB; r++) {
         const int cnt = a.sb_count[r + 1], mb = a.sb_mbase[r + 1];
         const int h = 1 << r;
+        if (STAG && cnt >= 2) {
 #pragma unroll
-        for (int u = 0; u < (STAG ? st_count(RB, r) : 0); u++) {
-            const int k = u >> r, j = u & (h - 1);
-            if (2 * k + 1 < cnt) {
-                const int qa = ((2 * k + 1) << r) | j, qb = ((2 * k + 2) << r) | j;
-                const int L = rt_lag(r, j);
-                float x = v[qa], y = v[qb];
-                float aa = (L == 0) ? x : lagged(x, ps[r][u], L, lane);
-                float bb = lagged(x, ps[r][u], L + 1, lane);
-                int m = mb + (2 * k + 1) * (2 << r) + 2 * bitrev_c(j, r);
-                emit(m, bfly(aa, y));
-                emit(m + 1, bfly(bb, y));
-                ps[r][u] = x;
+            for (int u = 0; u < (STAG ? st_count(RB, r) : 0); u++) {
+                const int k = u >> r, j = u & (h - 1);
+                if (2 * k + 1 < cnt) {
+                    const int qa = ((2 * k + 1) << r) | j, qb = ((2 * k + 2) << r) | j;
+                    const int L = rt_lag(r, j);
+                    float x = v[qa], y = v[qb];
+                    float aa = (L == 0) ? x : lagged(x, ps[r][u], L, lane);
+                    float bb = lagged(x, ps[r][u], L + 1, lane);
+                    int m = mb + (2 * k + 1) * (2 << r) + 2 * bitrev_c(j, r);
+                    emit(m, bfly(aa, y));
+                    emit(m + 1, bfly(bb, y));
+                    ps[r][u] = x;
+                }
             }
         }
 #pragma unroll
         for (int q = 0; q < RT<RB>::NP; q++) {
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
-            const int k = q >> r, j = q & (h - 1);
             const int L = rt_lag(r, q);
             if (EXT0 && r == 0) {
                 const float x = v[i0], y = v[i0 + 1];
@@ -422,11 +426,18 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
                 v[i0 + h] = bfly(bb, y);
                 pv[r][q] = x;
             }
-            const float o0 = v[i0], o1 = v[i0 + h];
-            if (2 * k < cnt) {
-                int m = mb + (2 * k) * (2 << r) + 2 * bitrev_c(j, r);
-                emit(m, o0);
-                emit(m + 1, o1);
+        }
+        // Even band pairs are step r's in-place outputs.
+        if (cnt > 0) {
+#pragma unroll
+            for (int q = 0; q < RT<RB>::NP; q++) {
+                const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
+                const int k = q >> r, j = q & (h - 1);
+                if (2 * k < cnt) {
+                    const int m = mb + (2 * k) * (2 << r) + 2 * bitrev_c(j, r);
+                    emit(m, v[i0]);
+                    emit(m + 1, v[i0 + h]);
+                }
             }
         }
     }
