@@ -838,6 +838,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
 
 constexpr int kPfWarps = 4;
 constexpr int kPfMaxLevels = 6;
+constexpr int kPfMaxProfiles = 16;   // 1 + 3 log2(max_width), max_width <= 32
 
 // Number of entries of boxcar level l in a window of len0 samples (level 0 = samples).
 __device__ __forceinline__ int pf_nlev(int len0, int l, int dt) { return (len0 - (1 << l)) / dt + 1; }
@@ -1027,6 +1028,7 @@ struct PfGeom
     int flags[kPfMaxLevels]; // kPfU: dt = 2^l; kPfPairs: scanned two fine samples at a time;
                              // kPfNextU: level l+1 has dt = 2^(l+1) and is built by this level's scan
     int raw_off;             // staging buffer of the window's raw samples (16-byte aligned)
+    int w_off;               // the warp's weights of one subband, [profile < 16][weight time < 32]
     int warp_floats;
 };
 
@@ -1099,7 +1101,8 @@ __host__ __device__ constexpr PfGeom pf_geom(int Dout, int Dcore, int tpad, int 
     }
     g.raw_off = (off + 3) & ~3;
     const int raw_floats = ((32 * Dout + tpad) * esize + 15) / 16 * 4;
-    g.warp_floats = g.raw_off + raw_floats;
+    g.w_off = g.raw_off + raw_floats;
+    g.warp_floats = g.w_off + kPfMaxProfiles * 32;
     return g;
 }
 
@@ -1130,7 +1133,14 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
     const int Dout = (DOUT > 0) ? DOUT : a.Dout;
     const int tpad = (DOUT > 0) ? pf_tpad_of(L) : a.tpad;
     const int Wds = a.ndm_out / a.ndm_wt, Tds = a.nt_out / a.nt_wt;
-    const float *wp = a.wt + ((((long) b * a.ndm_wt + dm / Wds) * a.nt_wt + (active ? tout / Tds : 0)) * a.P) * a.N;
+    // Weights of one subband for the warp's weight times tw0 .. tw0 + NT - 1, staged in shared memory
+    // as wsm[p * 32 + j] (lanes of one weight time read the same word, consecutive weight times
+    // consecutive words), and reloaded only when a multiplet's subband differs from the previous one.
+    const float *wrow = a.wt + ((long) b * a.ndm_wt + dm / Wds) * a.nt_wt * a.P * a.N;
+    const int tw0 = tout0 / Tds, NT = (Tds >= 32) ? 1 : 32 / Tds;
+    const int tl = active ? (tout / Tds - tw0) : 0;
+    float *wsm = lev + g.w_off;
+    int wsm_n = -1;
     const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
     const int mask = int(a.pf_cap - 1);
     // Window sample 0 (stream time s0 + 32 tile * Dout - tpad, a multiple of 4), as a delay-line slot.
@@ -1170,6 +1180,14 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
             stage(m + 1);
 
         const int n = a.m_to_n[m];
+        if (n != wsm_n) {
+            for (int idx = lane; idx < a.P * NT; idx += 32) {
+                const int p = idx / NT, j = idx - p * NT, t = tw0 + j;
+                wsm[p * 32 + j] = (t < a.nt_wt) ? wrow[((long) t * a.P + p) * a.N + n] : 0.0f;
+            }
+            __syncwarp();
+            wsm_n = n;
+        }
         bool upd = false;     // this lane's maximum moved to a group of this multiplet
         int winL = 0, winP = 0;
 #pragma unroll
@@ -1192,11 +1210,11 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
             }
 
             float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f;
-            if (l == 0) w0 = wp[n];
+            if (l == 0) w0 = wsm[tl];
             if (full) {
-                w1 = wp[(3 * l + 1) * a.N + n];
-                w2 = wp[(3 * l + 2) * a.N + n];
-                w3 = wp[(3 * l + 3) * a.N + n];
+                w1 = wsm[(3 * l + 1) * 32 + tl];
+                w2 = wsm[(3 * l + 2) * 32 + tl];
+                w3 = wsm[(3 * l + 3) * 32 + tl];
             }
 
             const int j0 = g.I[l] + lane * nsamp;
@@ -1302,10 +1320,10 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
                 const int l = winL;
                 const int dt = gr.dt[l], S = gr.S[l], nsamp = gr.nsamp[l];
                 const int j0 = gr.I[l] + lane * nsamp;
-                const float w0 = (l == 0) ? wp[n] : 0.0f;
-                const float w1 = full ? wp[(3 * l + 1) * a.N + n] : 0.0f;
-                const float w2 = full ? wp[(3 * l + 2) * a.N + n] : 0.0f;
-                const float w3 = full ? wp[(3 * l + 3) * a.N + n] : 0.0f;
+                const float w0 = (l == 0) ? wsm[tl] : 0.0f;
+                const float w1 = full ? wsm[(3 * l + 1) * 32 + tl] : 0.0f;
+                const float w2 = full ? wsm[(3 * l + 2) * 32 + tl] : 0.0f;
+                const float w3 = full ? wsm[(3 * l + 3) * 32 + tl] : 0.0f;
                 for (int is = winP; is < min(winP + 2, nsamp); is++) {
                     const int j = j0 + is;
                     const float x3 = lev[pf_phys(gr, l, j)];
@@ -1470,7 +1488,7 @@ int pf_warp_floats(int Dout, int tpad, int Dcore, int L)
 // The fast kernel needs 4-sample runs of the window (Dout >= 4, tpad and s0 multiples of 4).
 static bool pf_fast_ok(const PfArgs &a)
 {
-    return a.Dout >= 4 && (a.tpad % 4) == 0 && (a.s0 % 4) == 0 && (a.pf_cap % 4) == 0 && a.L <= 5;
+    return a.Dout >= 4 && (a.tpad % 4) == 0 && (a.s0 % 4) == 0 && (a.pf_cap % 4) == 0 && a.L <= 5 && a.P <= kPfMaxProfiles;
 }
 
 template<typename Ts, int L, int DOUT>
