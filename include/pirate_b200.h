@@ -106,6 +106,21 @@ int pb2_dd_allocate(pb2_dedisperser *dd);
 int pb2_dd_device_bytes(const pb2_dedisperser *dd, long *nbytes);
 /* GpuDedisperser::acquire_input, src_lib/GpuDedisperser.cpp:796; shape3 = (beams_per_batch, nfreq, nt_in) */
 int pb2_dd_acquire_input(pb2_dedisperser *dd, long seq_id, void *stream, void **ptr, long *shape3);
+/* int4 input, the raw format GpuDedisperser::time dequantizes into the input before dedispersing
+ * (src_lib/GpuDedisperser.cpp:1617-1660, GpuDequantizationKernel): acquires the next input slot as
+ * packed int4 data (beams_per_batch, nfreq, nt_in/2) bytes (two samples per byte, low nibble first)
+ * and fp16 (scale, offset) pairs (beams_per_batch, nfreq, nt_in/256, 2); same seq_id cursor as
+ * pb2_dd_acquire_input. pb2_dd_release_input then dequantizes inside the gridding kernel, with the
+ * same values pb2_dequantize would write in the config dtype. nt_in must be a multiple of 256. */
+int pb2_dd_acquire_input_int4(pb2_dedisperser *dd, long seq_id, void *stream, void **data, void **scales_offsets,
+                              long *shape3);
+/* GpuDequantizationKernel::launch (include/pirate/GpuDequantizationKernel.hpp:53-70) with
+ * ReferenceDequantizationKernel::apply's arithmetic (src_lib/GpuDequantizationKernel.cu:326-380):
+ * out = 0 where the int4 value is -8, else scale * value + offset in fp32, rounded once to out_dtype
+ * (0 float32, 1 float16, 2 bfloat16). Device arrays: out (nbeams, nfreq, ntime), scales_offsets
+ * (nbeams, nfreq, ntime/256, 2) fp16, data (nbeams, nfreq, ntime/2) bytes; ntime a multiple of 256. */
+int pb2_dequantize(void *out, int out_dtype, const void *scales_offsets, const void *data, long nbeams, long nfreq,
+                   long ntime, void *stream);
 /* GpuDedisperser::release_input_and_launch_dd_kernels, src_lib/GpuDedisperser.cpp:830 */
 int pb2_dd_release_input(pb2_dedisperser *dd, long seq_id, void *stream);
 /* GpuDedisperser::acquire_output, src_lib/GpuDedisperser.cpp:890 (sync != 0 blocks the host) */

@@ -1060,6 +1060,52 @@ static double test_lagbuf(uint64_t seed, long nrows, long nchunks, long ntime, l
 
 using namespace orc;
 
+// IEEE binary16 -> binary32, exact (every half is a float): sign, 5-bit exponent (bias 15), 10-bit
+// fraction; subnormals are normalized, infinities and NaNs keep their class.
+static float orc_half_to_float(uint16_t h)
+{
+    const uint32_t sign = uint32_t(h >> 15) << 31;
+    const uint32_t e = (h >> 10) & 0x1f, frac = h & 0x3ff;
+    uint32_t bits;
+    if (e == 0x1f) {
+        bits = sign | 0x7f800000u | (frac << 13);
+    } else if (e != 0) {
+        bits = sign | ((e - 15 + 127) << 23) | (frac << 13);
+    } else if (frac == 0) {
+        bits = sign;
+    } else {
+        int ee = -14;                 // value = frac * 2^-24 = 1.f * 2^(ee)
+        uint32_t m = frac;
+        while (!(m & 0x400)) { m <<= 1; ee--; }
+        bits = sign | (uint32_t(ee + 127) << 23) | ((m & 0x3ff) << 13);
+    }
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f;
+}
+
+// ReferenceDequantizationKernel::apply (src_lib/GpuDequantizationKernel.cu:326-380): int4 data
+// (low nibble = even sample), one fp16 (scale, offset) pair per 256 samples of a (beam, freq) row,
+// out = 0 for the sentinel -8, else scale * value + offset in fp32 (a multiply, then an add).
+static void orc_dequantize_impl(const uint8_t *data, const uint16_t *scoff, float *out, long nbeams, long nfreq, long ntime)
+{
+    const long nchunks = ntime / 256;
+    for (long row = 0; row < nbeams * nfreq; row++) {
+        for (long c = 0; c < nchunks; c++) {
+            const long pair = row * nchunks + c;
+            const float scale = orc_half_to_float(scoff[2 * pair]), offset = orc_half_to_float(scoff[2 * pair + 1]);
+            for (long it = 0; it < 256; it++) {
+                const long i = (row * nchunks + c) * 256 + it;
+                const uint8_t byte = data[i / 2];
+                const int nib = (i % 2 == 0) ? (byte & 0x0f) : ((byte >> 4) & 0x0f);
+                const int value = (nib >= 8) ? (nib - 16) : nib;
+                const float prod = scale * float(value);
+                out[i] = (value == -8) ? 0.0f : (prod + offset);
+            }
+        }
+    }
+}
+
 struct orc_handle
 {
     int real_bits;
@@ -1073,6 +1119,15 @@ static thread_local std::string orc_err;
 extern "C" {
 
 const char *orc_last_error() { return orc_err.c_str(); }
+
+int orc_dequantize(const uint8_t *data, const uint16_t *scales_offsets, float *out, long nbeams, long nfreq, long ntime)
+{
+    if (ntime % 256) { orc_err = "orc_dequantize: ntime must be a multiple of 256"; return -1; }
+    orc_dequantize_impl(data, scales_offsets, out, nbeams, nfreq, ntime);
+    return 0;
+}
+
+float orc_half_to_float_c(uint16_t h) { return orc_half_to_float(h); }
 
 // Primary tree i: ptrees[6*i .. 6*i+5] = (num_early_triggers, max_width, dm_downsampling,
 // time_downsampling, wt_dm_downsampling, wt_time_downsampling).

@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-__all__ = ["DedispersionConfig", "DedispersionPlan", "GpuDedisperser", "Outputs", "lib", "LIB_PATH"]
+__all__ = ["DedispersionConfig", "DedispersionPlan", "GpuDedisperser", "Outputs", "dequantize", "lib", "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 # The in-tree build; PB2_LIBRARY names another build of the same library (for example one made with
@@ -81,6 +81,8 @@ def lib():
         "pb2_dd_device_bytes": (ctypes.c_int, [vp, lp]),
         "pb2_dd_acquire_input": (ctypes.c_int, [vp, ctypes.c_long, vp, ctypes.POINTER(vp), lp]),
         "pb2_dd_release_input": (ctypes.c_int, [vp, ctypes.c_long, vp]),
+        "pb2_dd_acquire_input_int4": (ctypes.c_int, [vp, ctypes.c_long, vp, ctypes.POINTER(vp), ctypes.POINTER(vp), lp]),
+        "pb2_dequantize": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, vp]),
         "pb2_dd_acquire_output": (ctypes.c_int, [vp, ctypes.c_long, ctypes.c_long, vp, ctypes.c_int, ctypes.POINTER(_Outputs)]),
         "pb2_dd_release_output": (ctypes.c_int, [vp, ctypes.c_long, ctypes.c_long, vp]),
         "pb2_dd_fill_weights": (ctypes.c_int, [vp, ctypes.c_long, vp, ctypes.c_long]),
@@ -358,6 +360,20 @@ class GpuDedisperser:
         return _device_tensor(ptr.value, tuple(shape), {"float32": "float32", "float16": "float16",
                                                         "bfloat16": "bfloat16"}[self.dtype], self.device)
 
+    def acquire_input_int4(self, seq_id, stream=None):
+        """The next input slot in pirate's raw format: returns (data, scales_offsets), device tensors of
+        shapes (B, nfreq, nt_in // 2) uint8 (two int4 samples per byte, low nibble first) and
+        (B, nfreq, nt_in // 256, 2) float16 (scale, offset). Same seq_id cursor as acquire_input; the
+        kernels dequantize while gridding (GpuDedisperser::time's input, src_lib/GpuDedisperser.cpp:1617-1660)."""
+        data = ctypes.c_void_p()
+        so = ctypes.c_void_p()
+        shape = (ctypes.c_long * 3)()
+        _check(lib().pb2_dd_acquire_input_int4(self._h, int(seq_id), _stream_ptr(stream), ctypes.byref(data),
+                                               ctypes.byref(so), shape))
+        B, F, T = tuple(shape)
+        return (_device_tensor(data.value, (B, F, T // 2), "uint8", self.device),
+                _device_tensor(so.value, (B, F, T // 256, 2), "float16", self.device))
+
     def release_input_and_launch_dd_kernels(self, seq_id, stream=None):
         _check(lib().pb2_dd_release_input(self._h, int(seq_id), _stream_ptr(stream)))
 
@@ -389,6 +405,16 @@ class GpuDedisperser:
         self._next_in += 1
 
     @contextlib.contextmanager
+    def get_input_int4(self, stream=None):
+        """Context manager: yields (data, scales_offsets) of the next input slot in int4 form, then
+        launches the kernels on exit."""
+        seq = self._next_in
+        arrs = self.acquire_input_int4(seq, stream)
+        yield arrs
+        self.release_input_and_launch_dd_kernels(seq, stream)
+        self._next_in += 1
+
+    @contextlib.contextmanager
     def get_output(self, consumer_id=0, stream=None, sync=False):
         """Context manager: yields the next Outputs for 'consumer_id', released on exit."""
         seq = self._next_out[consumer_id]
@@ -401,3 +427,24 @@ class GpuDedisperser:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.pb2_dd_destroy(self._h)
             self._h = None
+
+
+def dequantize(out, scales_offsets, data, stream=None):
+    """pirate's GpuDequantizationKernel::launch (include/pirate/GpuDequantizationKernel.hpp:53-70) on
+    torch device tensors: out (nbeams, nfreq, ntime) float32/float16/bfloat16, scales_offsets
+    (nbeams, nfreq, ntime // 256, 2) float16, data (nbeams, nfreq, ntime // 2) uint8. out = 0 where the
+    int4 value is -8, else scale * value + offset in fp32, rounded once to out's dtype."""
+    import torch
+    codes = {torch.float32: 0, torch.float16: 1, torch.bfloat16: 2}
+    if out.dtype not in codes:
+        raise RuntimeError("dequantize: out must be float32, float16 or bfloat16")
+    nbeams, nfreq, ntime = out.shape
+    if tuple(data.shape) != (nbeams, nfreq, ntime // 2) or data.dtype != torch.uint8:
+        raise RuntimeError("dequantize: data must be uint8 of shape (nbeams, nfreq, ntime // 2)")
+    if tuple(scales_offsets.shape) != (nbeams, nfreq, ntime // 256, 2) or scales_offsets.dtype != torch.float16:
+        raise RuntimeError("dequantize: scales_offsets must be float16 of shape (nbeams, nfreq, ntime // 256, 2)")
+    for t in (out, scales_offsets, data):
+        if not (t.is_cuda and t.is_contiguous()):
+            raise RuntimeError("dequantize: arrays must be contiguous CUDA tensors")
+    _check(lib().pb2_dequantize(out.data_ptr(), codes[out.dtype], scales_offsets.data_ptr(), data.data_ptr(),
+                                nbeams, nfreq, ntime, _stream_ptr(stream)))

@@ -212,6 +212,30 @@ int pb2_dd_acquire_input(pb2_dedisperser *dd, long seq_id, void *stream, void **
     });
 }
 
+int pb2_dd_acquire_input_int4(pb2_dedisperser *dd, long seq_id, void *stream, void **data, void **scales_offsets, long *shape3)
+{
+    return guard([&] {
+        REQUIRE_PTR(dd); REQUIRE_PTR(data); REQUIRE_PTR(scales_offsets);
+        *data = dd->d->acquire_input_int4(seq_id, (cudaStream_t) stream, scales_offsets);
+        if (shape3) {
+            shape3[0] = dd->d->plan.beams_per_batch;
+            shape3[1] = dd->d->plan.nfreq;
+            shape3[2] = dd->d->plan.nt_in;
+        }
+    });
+}
+
+int pb2_dequantize(void *out, int out_dtype, const void *scales_offsets, const void *data, long nbeams, long nfreq,
+                   long ntime, void *stream)
+{
+    return guard([&] {
+        REQUIRE_PTR(out); REQUIRE_PTR(scales_offsets); REQUIRE_PTR(data);
+        if (out_dtype < 0 || out_dtype > 2) throw std::runtime_error("pb2_dequantize: out_dtype must be 0 (float32), 1 (float16) or 2 (bfloat16)");
+        if (nbeams < 0 || nfreq < 0) throw std::runtime_error("pb2_dequantize: negative shape");
+        pb2::launch_dequantize(out, out_dtype, data, scales_offsets, nbeams, nfreq, ntime, (cudaStream_t) stream);
+    });
+}
+
 int pb2_dd_release_input(pb2_dedisperser *dd, long seq_id, void *stream)
 {
     return guard([&] { REQUIRE_PTR(dd); dd->d->release_input_and_launch_dd_kernels(seq_id, (cudaStream_t) stream); });

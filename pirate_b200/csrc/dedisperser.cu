@@ -226,6 +226,11 @@ void GpuDedisperser::allocate()
         d_grid_w.upload(w.data(), w.size() * 4);
 
         add(d_inputs, size_t(nslots_in) * B * F * nt * esize);
+        if (nt % 256 == 0) {
+            add(d_qdata, size_t(nslots_in) * B * F * (nt / 2));
+            add(d_qscoff, size_t(nslots_in) * B * F * (nt / 256) * 2 * sizeof(uint16_t));
+        }
+        slot_int4.assign(nslots_in, false);
         add(d_tree0, size_t(B) * N * nt * esize);
         if (npri > 1) add(d_lds_state, size_t(2) * total_beams * (npri - 1) * (N / 2) * sizeof(float));
 
@@ -310,13 +315,32 @@ void GpuDedisperser::allocate()
 
 void *GpuDedisperser::acquire_input(long seq_id, cudaStream_t stream)
 {
+    return acquire_slot(seq_id, stream, nullptr);
+}
+
+void *GpuDedisperser::acquire_input_int4(long seq_id, cudaStream_t stream, void **scales_offsets)
+{
+    if (!scales_offsets) throw runtime_error("GpuDedisperser::acquire_input_int4(): null scales_offsets");
+    return acquire_slot(seq_id, stream, scales_offsets);
+}
+
+// int4 != nullptr: acquire the slot's int4 buffers (data returned, scales/offsets in *int4).
+void *GpuDedisperser::acquire_slot(long seq_id, cudaStream_t stream, void **int4)
+{
     return entry([&]() -> void * {
         if (!allocated) throw runtime_error("GpuDedisperser::acquire_input(): allocate() was not called");
         if (seq_id != next_acq_in)
             throw runtime_error("GpuDedisperser::acquire_input(): expected seq_id=" + std::to_string(next_acq_in) + ", got " + std::to_string(seq_id));
+        if (int4 && !d_qdata.ptr)
+            throw runtime_error("GpuDedisperser::acquire_input_int4(): time_samples_per_chunk must be a multiple of 256");
         long slot = seq_id % nslots_in;
         if (in_free_recorded[slot]) CUDA_CHECK(cudaStreamWaitEvent(stream, ev_in_free[slot], 0));
         next_acq_in++;
+        slot_int4[slot] = (int4 != nullptr);
+        if (int4) {
+            *int4 = d_qscoff.as<char>() + size_t(slot) * B * plan.nfreq * (plan.nt_in / 256) * 2 * sizeof(uint16_t);
+            return d_qdata.as<char>() + size_t(slot) * B * plan.nfreq * (plan.nt_in / 2);
+        }
         return d_inputs.as<char>() + size_t(slot) * B * plan.nfreq * plan.nt_in * esize;
     });
 }
@@ -347,6 +371,10 @@ void GpuDedisperser::launch_batch(long seq_id)
     GridLdsArgs g;
     memset(&g, 0, sizeof(g));
     g.in = d_inputs.as<char>() + size_t(slot_in) * B * F * nt * esize;
+    if (slot_int4[slot_in]) {
+        g.q_data = d_qdata.as<char>() + size_t(slot_in) * B * F * (nt / 2);
+        g.q_scoff = d_qscoff.as<char>() + size_t(slot_in) * B * F * (nt / 256) * 2 * sizeof(uint16_t);
+    }
     g.tree0 = d_tree0.ptr;
     g.chan_f0 = d_grid_f0.as<int>();
     g.chan_cnt = d_grid_cnt.as<int>();

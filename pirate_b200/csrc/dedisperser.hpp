@@ -7,6 +7,7 @@
 //
 // Device memory layout (all allocated and zeroed by allocate()):
 //   inputs    nslots_in x (B, nfreq, nt_in)                     storage dtype
+//   int4 in   nslots_in x (B, nfreq, nt_in/2) bytes + (B, nfreq, nt_in/256, 2) fp16 scales/offsets
 //   tree0     (B, 2^rank, nt_in) level-0 tree                    storage dtype
 //   lds[p]    (total_beams, 2^(rank-1), cap_p) delay lines       storage dtype, cap_p = 2^k >= nt_p + 2^s1dd - 1
 //   ring[p]   per stage-1 output row (a, dm_brev): a delay line of capacity max_lag(row) + nt_p (rounded to 32)
@@ -70,6 +71,10 @@ public:
 
     void allocate();
     void *acquire_input(long seq_id, cudaStream_t stream);
+    // The next input slot as int4 data (B, nfreq, nt/2) bytes; *scales_offsets receives its fp16
+    // (scale, offset) pairs (B, nfreq, nt/256, 2). Same cursor as acquire_input. The gridding kernel
+    // then dequantizes while it reads (nt must be a multiple of 256).
+    void *acquire_input_int4(long seq_id, cudaStream_t stream, void **scales_offsets);
     void release_input_and_launch_dd_kernels(long seq_id, cudaStream_t stream);
     Outputs acquire_output(long consumer_id, long seq_id, cudaStream_t stream, bool sync);
     void release_output(long consumer_id, long seq_id, cudaStream_t stream);
@@ -113,6 +118,7 @@ private:
 
     // Per-slot events.
     std::vector<cudaEvent_t> ev_in_acquired, ev_in_free, ev_out_done;
+    std::vector<bool> slot_int4;   // input slot holds int4 data (acquire_input_int4)
     std::vector<std::vector<cudaEvent_t>> ev_out_released;   // [consumer][slot]
     std::vector<bool> in_free_recorded, out_done_recorded;
     std::vector<std::vector<bool>> out_released_recorded;
@@ -145,6 +151,8 @@ private:
     std::vector<Stage1> s1;
     std::vector<Stage2> s2;
     DeviceBuffer d_inputs, d_tree0, d_lds_state;
+    DeviceBuffer d_qdata, d_qscoff;   // int4 input slots (allocated when nt is a multiple of 256)
+    void *acquire_slot(long seq_id, cudaStream_t stream, void **int4);
 };
 
 }  // namespace pb2

@@ -132,25 +132,96 @@ __device__ __forceinline__ void store_run(Ts *p, const float (&o)[W])
     }
 }
 
-// Grids tree channel n over samples [t0, t0+W) of one beam's input (xb = beam base).
+// int4 dequantization, restating pirate's ReferenceDequantizationKernel::apply
+// (src_lib/GpuDequantizationKernel.cu:326-380): nibble -> signed value v in [-8, 7]; v = -8 is the
+// "missing sample" sentinel and gives 0; otherwise scale * v + offset, one fp32 multiply and one fp32
+// add with (scale, offset) converted from fp16. The result is then rounded once to the output type.
+__device__ __forceinline__ float dq_value(uint32_t nib, float scale, float offset)
+{
+    const int v = int(nib & 0xf) - int((nib & 8) << 1);
+    return (v == -8) ? 0.0f : __fadd_rn(__fmul_rn(scale, float(v)), offset);
+}
+
+// W consecutive samples from t0 of one int4 row (row = the row's bytes, so = its (scale, offset)
+// pairs), dequantized, rounded to Ts and returned as floats. The W samples lie in one 256-sample
+// scale block; for W >= 8, t0 is a multiple of 8 (32-bit nibble words).
 template<typename Ts, int W>
-__device__ __forceinline__ void grid_run(const GridLdsArgs &a, const Ts *xb, long n, long t0, float (&o)[W])
+__device__ __forceinline__ void load_run_q(const uint8_t *row, const __half2 *so_row, long t0, float (&o)[W])
+{
+    const float2 so = __half22float2(so_row[t0 >> 8]);
+    if constexpr (W % 8 == 0) {
+#pragma unroll
+        for (int w = 0; w < W / 8; w++) {
+            const uint32_t word = ((const uint32_t *) (row + (t0 >> 1)))[w];
+#pragma unroll
+            for (int k = 0; k < 8; k++) o[8 * w + k] = to_f(from_f<Ts>(dq_value(word >> (4 * k), so.x, so.y)));
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < W; i++) {
+            const long t = t0 + i;
+            const uint32_t byte = row[t >> 1];
+            o[i] = to_f(from_f<Ts>(dq_value((t & 1) ? (byte >> 4) : byte, so.x, so.y)));
+        }
+    }
+}
+
+// Grids tree channel n over samples [t0, t0+W) of batch beam b's input. With Q the input rows are
+// int4 (dequantized on load exactly as the standalone dequantization kernel would write them).
+template<typename Ts, int W, bool Q>
+__device__ __forceinline__ void grid_run(const GridLdsArgs &a, int b, long n, long t0, float (&o)[W])
 {
 #pragma unroll
     for (int i = 0; i < W; i++) o[i] = 0.0f;
     const int f0 = a.chan_f0[n], cnt = a.chan_cnt[n], woff = a.chan_woff[n];
     for (int k = 0; k < cnt; k++) {
         const float w = a.chan_w[woff + k];
+        const long row = (long) b * a.F + f0 + k;
         float x[W];
-        load_run<Ts, W>(xb + (long) (f0 + k) * a.T + t0, x);
+        if constexpr (Q)
+            load_run_q<Ts, W>((const uint8_t *) a.q_data + row * (a.T >> 1), (const __half2 *) a.q_scoff + row * (a.T >> 8), t0, x);
+        else
+            load_run<Ts, W>((const Ts *) a.in + row * a.T + t0, x);
 #pragma unroll
         for (int i = 0; i < W; i++) o[i] = __fadd_rn(o[i], __fmul_rn(w, x[i]));
     }
 }
 
+// Standalone dequantization: one thread per 32 samples (16 input bytes, 16-byte output stores).
+template<typename To>
+__global__ void __launch_bounds__(256) dequant_kernel(To *out, const uint8_t *data, const __half2 *scoff, long rows, int T)
+{
+    const long nper = T / 32;
+    const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= rows * nper)
+        return;
+    const long row = g / nper;
+    const long t0 = (g - row * nper) * 32;
+    float o[32];
+    load_run_q<To, 32>(data + row * (T >> 1), scoff + row * (T >> 8), t0, o);
+    store_run<To, 32>(out + row * T + t0, o);
+}
+
+void launch_dequantize(void *out, int out_dtype, const void *data, const void *scales_offsets, long nbeams, long nfreq,
+                       long ntime, cudaStream_t s)
+{
+    if (ntime <= 0 || ntime % 256) throw std::runtime_error("dequantize: ntime must be a positive multiple of 256");
+    if (!out || !data || !scales_offsets) throw std::runtime_error("dequantize: null pointer");
+    const long rows = nbeams * nfreq;
+    const long nthr = rows * (ntime / 32);
+    if (nthr == 0) return;
+    const unsigned grid = (unsigned) ((nthr + 255) / 256);
+    const uint8_t *d = (const uint8_t *) data;
+    const __half2 *so = (const __half2 *) scales_offsets;
+    if (out_dtype == 0) dequant_kernel<float><<<grid, 256, 0, s>>>((float *) out, d, so, rows, int(ntime));
+    else if (out_dtype == 1) dequant_kernel<__half><<<grid, 256, 0, s>>>((__half *) out, d, so, rows, int(ntime));
+    else dequant_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>((__nv_bfloat16 *) out, d, so, rows, int(ntime));
+    check_launch("dequant_kernel");
+}
+
 constexpr int kGridMaxThreads = 512;
 
-template<typename Ts, int NLEV>
+template<typename Ts, int NLEV, bool Q>
 __global__ void __launch_bounds__(kGridMaxThreads) grid_lds_kernel(GridLdsArgs a)
 {
     constexpr int W0 = ((1 << NLEV) > 8) ? (1 << NLEV) : 8;
@@ -170,11 +241,10 @@ __global__ void __launch_bounds__(kGridMaxThreads) grid_lds_kernel(GridLdsArgs a
     const int parity = int(a.ichunk & 1);
     const long t0 = (long) win * W0;
 
-    const Ts *xb = (const Ts *) a.in + (long) b * a.F * a.T;
     float r0[W0], r1[W0];
     if (live) {
-        grid_run<Ts, W0>(a, xb, 2 * c, t0, r0);
-        grid_run<Ts, W0>(a, xb, 2 * c + 1, t0, r1);
+        grid_run<Ts, W0, Q>(a, b, 2 * c, t0, r0);
+        grid_run<Ts, W0, Q>(a, b, 2 * c + 1, t0, r1);
         Ts *lev0 = (Ts *) a.tree0 + ((long) b * (2 * nhalf) + 2 * c) * a.T + t0;
         store_run<Ts, W0>(lev0, r0);
         store_run<Ts, W0>(lev0 + a.T, r1);
@@ -228,7 +298,7 @@ __global__ void __launch_bounds__(kGridMaxThreads) grid_lds_kernel(GridLdsArgs a
             } else {
                 // The previous window belongs to the previous block: grid its WE samples again.
                 float e[WE];
-                grid_run<Ts, WE>(a, xb, 2 * c, t0 - WE, e);
+                grid_run<Ts, WE, Q>(a, b, 2 * c, t0 - WE, e);
 #pragma unroll
                 for (int p = 1; p <= NLEV; p++) {
 #pragma unroll
@@ -1385,7 +1455,12 @@ static void launch_grid_lds_t(const GridLdsArgs &a, cudaStream_t s)
     // Blocks start at a window 0 (a multiple of nwin threads, about 128), so that every other window's
     // predecessor is computed in the same block.
     int bd = (nwin <= 128) ? int(nwin * (128 / nwin)) : (nwin <= kGridMaxThreads ? int(nwin) : kGridMaxThreads);
-    grid_lds_kernel<Ts, NLEV><<<(unsigned) ((nthr + bd - 1) / bd), bd, 0, s>>>(a);
+    if (a.q_data) {
+        if (a.T % 256) throw std::runtime_error("grid_lds_kernel: int4 input needs a chunk length that is a multiple of 256");
+        grid_lds_kernel<Ts, NLEV, true><<<(unsigned) ((nthr + bd - 1) / bd), bd, 0, s>>>(a);
+    } else {
+        grid_lds_kernel<Ts, NLEV, false><<<(unsigned) ((nthr + bd - 1) / bd), bd, 0, s>>>(a);
+    }
     check_launch("grid_lds_kernel");
 }
 

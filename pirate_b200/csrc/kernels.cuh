@@ -109,6 +109,10 @@ struct GridLdsArgs
     int lag_rank;           // output row c is written delayed by 2^lag_rank - 1 - (c mod 2^lag_rank) samples
     long ichunk;
     int beam0, B, total_beams;
+    // int4 input in place of 'in' (null when the input is in the storage dtype): q_data (B, F, T/2)
+    // bytes, two samples per byte (low nibble first); q_scoff (B, F, T/256, 2) fp16 (scale, offset).
+    const void *q_data;
+    const void *q_scoff;
 };
 
 // Floats of persistent state per block of the stage kernels (host and device agree by construction).
@@ -116,6 +120,9 @@ inline long stage1_state_floats(int R) { return tree_state_floats(split_ra(R), s
 inline long stage2_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), true); }
 
 void launch_grid_lds(const GridLdsArgs &a, int dtype, cudaStream_t s);
+// int4 -> out_dtype dequantization of (nbeams, nfreq, ntime) samples (ntime a multiple of 256).
+void launch_dequantize(void *out, int out_dtype, const void *data, const void *scales_offsets, long nbeams, long nfreq,
+                       long ntime, cudaStream_t s);
 void launch_stage1(const Stage1Args &a, int dtype, int nblocks, int B, cudaStream_t s);
 void launch_stage2(const Stage2Args &a, int dtype, int nblocks, int B, cudaStream_t s);
 void launch_pf(const PfArgs &a, int dtype, int B, cudaStream_t s);

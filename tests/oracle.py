@@ -59,6 +59,10 @@ def lib():
         L.orc_test_lagbuf.argtypes = [ctypes.c_uint64] + [ctypes.c_long] * 4
         L.orc_subbands.argtypes = [ctypes.c_int, c_long_p, c_long_p, c_long_p, c_long_p, c_long_p, c_long_p]
         L.orc_restrict_subbands.argtypes = [ctypes.c_int, c_long_p, ctypes.c_long, ctypes.c_long, c_long_p]
+        L.orc_dequantize.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
+                                     ctypes.c_long, ctypes.c_long]
+        L.orc_half_to_float_c.restype = ctypes.c_float
+        L.orc_half_to_float_c.argtypes = [ctypes.c_uint16]
         _lib = L
     return _lib
 
@@ -230,3 +234,29 @@ def random_weights(shape, rng):
     r = rng.uniform(0, 1, size=shape)
     x = rng.uniform(0, 1, size=shape)
     return np.where(r < p0, x, 0.0).astype(np.float32)
+
+
+def dequantize(data_u8, scales_offsets_f16, nbeams, nfreq, ntime):
+    """ReferenceDequantizationKernel::apply (src_lib/GpuDequantizationKernel.cu:326-380), fp32 output.
+    data_u8: (nbeams, nfreq, ntime // 2) uint8, two int4 samples per byte (low nibble first);
+    scales_offsets_f16: (nbeams, nfreq, ntime // 256, 2) float16 (scale, offset)."""
+    d = np.ascontiguousarray(data_u8, dtype=np.uint8)
+    so = np.ascontiguousarray(scales_offsets_f16, dtype=np.float16)
+    out = np.empty((nbeams, nfreq, ntime), np.float32)
+    if lib().orc_dequantize(d.ctypes.data, so.ctypes.data, out.ctypes.data, nbeams, nfreq, ntime) != 0:
+        raise RuntimeError(_err())
+    return out
+
+
+def random_quantized(rng, nbeams, nfreq, ntime, missing=0.01):
+    """Seeded int4 data (two samples per byte, a fraction 'missing' of -8 sentinels) and fp16
+    (scale, offset) pairs: scales in [0, 1], offsets in [-1, 1], as pirate's test
+    (src_lib/GpuDequantizationKernel.cu:508-515)."""
+    v = rng.integers(-7, 8, size=(nbeams, nfreq, ntime))
+    v[rng.random(v.shape) < missing] = -8
+    nib = (v & 0xf).astype(np.uint8)
+    data = (nib[..., 0::2] | (nib[..., 1::2] << 4)).astype(np.uint8)
+    so = np.empty((nbeams, nfreq, ntime // 256, 2), np.float16)
+    so[..., 0] = rng.uniform(0.0, 1.0, so.shape[:-1])
+    so[..., 1] = rng.uniform(-1.0, 1.0, so.shape[:-1])
+    return data, so
