@@ -128,6 +128,7 @@ def run_ours(args, rank, world):
     import numpy as np
     import torch
     import pirate_b200 as pb
+    from pirate_b200 import replicas
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
@@ -184,8 +185,7 @@ def run_ours(args, rank, world):
     for _ in range(args.warmup):
         step_device()
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
 
     dd.enable_timing(True)
@@ -201,12 +201,8 @@ def run_ours(args, rank, world):
         clk.mark(h0, time.time())
     ktimes = dd.kernel_times()
     dd.enable_timing(False)
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        torch.distributed.barrier()
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1))
+    replicas.barrier()
     ms_per_step = ms / args.steps
 
     # End to end through the public API, as pirate's timing loop (GpuDedisperser::time,
@@ -251,8 +247,7 @@ def run_ours(args, rank, world):
     for _ in range(3):
         step_e2e()
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    replicas.barrier()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(copy_stream)
@@ -260,11 +255,7 @@ def run_ours(args, rank, world):
         step_e2e()
     f1.record(out_stream)
     torch.cuda.synchronize()
-    ems = f0.elapsed_time(f1)
-    if world > 1:
-        t = torch.tensor([ems], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ems = float(t.item())
+    ems = replicas.max_over_ranks(f0.elapsed_time(f1))
 
     alg = dd.algorithmic_bytes()
     # The gridding class reads int4 data and scales/offsets instead of storage-dtype samples.
@@ -387,9 +378,9 @@ def main():
 
     r = run_ours(args, rank, world)
     peak, peak_kind = load_peaks()
-    nbeams_total = args.beams * world
-    value = nbeams_total * CHUNK_SECONDS / (r["ms_per_step"] * 1e-3)
-    e2e = nbeams_total * CHUNK_SECONDS / (r["e2e_ms_per_step"] * 1e-3)
+    from pirate_b200.replicas import real_time_beams
+    value = real_time_beams(args.beams, world, r["ms_per_step"] * 1e-3, CHUNK_SECONDS)
+    e2e = real_time_beams(args.beams, world, r["e2e_ms_per_step"] * 1e-3, CHUNK_SECONDS)
 
     classes = ["grid_lds", "unused", "stage1", "stage2", "pf"]
     kt = r["ktimes"]
