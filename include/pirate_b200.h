@@ -67,6 +67,15 @@ int pb2_plan_to_yaml(const pb2_plan *plan, char *buf, long buflen, long *needed)
 /* DedispersionPlan::ntrees / trees[i] (include/pirate/DedispersionTree.hpp:19-59) */
 int pb2_plan_ntrees(const pb2_plan *plan, long *ntrees);
 int pb2_plan_tree_info(const pb2_plan *plan, long itree, pb2_tree_info *out);
+/* DedispersionTree::frequency_subbands.n_to_flo / n_to_fhi (include/pirate/FrequencySubbands.hpp):
+ * the peak-finding frequency-band range [flo, fhi) of each of the tree's n == N subbands. */
+int pb2_plan_tree_subbands(const pb2_plan *plan, long itree, long *n_to_flo, long *n_to_fhi, long n);
+/* PfAvarApproximation(plan, freq_variances).tree_variance, include/pirate/PfVariance.hpp:86-120,
+ * src_lib/PfVariance.cpp:236-337: analytic variance of each peak-finding trial under unit weights
+ * for white-noise input of per-channel variance freq_variances[nfreq] (all > 0). out[itree] receives
+ * tree itree's (N, ndm_wt, nprofiles) doubles, out_len[itree] = N * ndm_wt * nprofiles. */
+int pb2_plan_pf_variances(const pb2_plan *plan, const double *freq_variances, long nfreq, double *const *out,
+                          const long *out_len, long ntrees);
 /* DedispersionPlan::stage1_dd_rank / stage1_amb_rank (length num_primary_trees) */
 int pb2_plan_stage1_ranks(const pb2_plan *plan, long *dd_rank, long *amb_rank, long n);
 /* DedispersionPlan::decode_argmax, src_lib/DedispersionPlan.cpp:481; out5 = (fmin, fmax, tlo, thi, p) */
@@ -130,6 +139,11 @@ int pb2_dd_release_output(pb2_dedisperser *dd, long consumer_id, long seq_id, vo
 /* GpuDedisperser::fill_all_weights, src_lib/GpuDedisperser.cpp:1240; host array
  * (nbatches_wt, beams_per_batch, ndm_wt, nt_wt, nprofiles, N) float32 */
 int pb2_dd_fill_weights(pb2_dedisperser *dd, long itree, const float *host, long nelts);
+/* GpuDedisperser::fill_analytic_weights, include/pirate/Dedisperser.hpp:237-244,
+ * src_lib/GpuDedisperser.cpp:1162-1238: every weight slot and beam of every tree gets
+ * 1/sqrt(variance) of PfAvarApproximation (see pb2_plan_pf_variances) for the per-channel input
+ * variances freq_variances[nfreq] (all > 0). Blocks until the weights are on the GPU. */
+int pb2_dd_fill_analytic_weights(pb2_dedisperser *dd, const double *freq_variances, long nfreq);
 /* GpuDedisperser::stop, src_lib/GpuDedisperser.cpp:735 */
 int pb2_dd_stop(pb2_dedisperser *dd);
 /* Kernel launches per (chunk, batch), and algorithmic HBM bytes per (chunk, batch) for the

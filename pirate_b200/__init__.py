@@ -14,7 +14,8 @@ import os
 
 import numpy as np
 
-__all__ = ["DedispersionConfig", "DedispersionPlan", "GpuDedisperser", "Outputs", "dequantize", "lib", "LIB_PATH"]
+__all__ = ["DedispersionConfig", "DedispersionPlan", "GpuDedisperser", "Outputs", "PfAvarApproximation", "dequantize",
+           "lib", "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 # The in-tree build; PB2_LIBRARY names another build of the same library (for example one made with
@@ -76,6 +77,9 @@ def lib():
         "pb2_plan_decode_argmax": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_long, ctypes.c_long, ctypes.c_long, lp]),
         "pb2_plan_decode_argmax2": (ctypes.c_int, [vp, ctypes.c_long, lp, dp]),
         "pb2_plan_steady_state_it0": (ctypes.c_int, [vp, ctypes.c_long, lp, ctypes.c_long]),
+        "pb2_plan_tree_subbands": (ctypes.c_int, [vp, ctypes.c_long, lp, lp, ctypes.c_long]),
+        "pb2_plan_pf_variances": (ctypes.c_int, [vp, dp, ctypes.c_long, ctypes.POINTER(dp), lp, ctypes.c_long]),
+        "pb2_dd_fill_analytic_weights": (ctypes.c_int, [vp, dp, ctypes.c_long]),
         "pb2_dd_create": (ctypes.c_int, [vp, ctypes.POINTER(_DdParams), ctypes.POINTER(vp)]),
         "pb2_dd_allocate": (ctypes.c_int, [vp]),
         "pb2_dd_device_bytes": (ctypes.c_int, [vp, lp]),
@@ -162,6 +166,16 @@ class DedispersionConfig:
     def get_total_nfreq(self):
         return int(sum(self._d["zone_nfreq"]))
 
+    def make_random_freq_variances(self, noisy=False, rng=None):
+        """Per-channel input variances for tests (DedispersionConfig::make_random_freq_variances,
+        src_lib/DedispersionConfig.cpp:253-272): one uniform random value in (0, 1) per zone,
+        repeated over the zone's channels. rng: a numpy Generator (default: a fresh one)."""
+        rng = np.random.default_rng() if rng is None else rng
+        zone_var = [float(rng.uniform(1e-6, 1.0)) for _ in self._d["zone_nfreq"]]
+        if noisy:
+            print("make_random_freq_variances: per-zone variances = %s" % (tuple(zone_var),))
+        return np.concatenate([np.full(int(n), v) for n, v in zip(self._d["zone_nfreq"], zone_var)])
+
     def make_channel_map(self):
         n = 2 ** int(self._d["toplevel_tree_rank"]) + 1
         out = np.zeros(n, dtype=np.float64)
@@ -220,7 +234,12 @@ class DedispersionPlan:
         for i in range(self.ntrees):
             info = _TreeInfo()
             _check(lib().pb2_plan_tree_info(h, i, ctypes.byref(info)))
-            self.trees.append(DedispersionTree(info))
+            tree = DedispersionTree(info)
+            flo = (ctypes.c_long * info.nsubbands)()
+            fhi = (ctypes.c_long * info.nsubbands)()
+            _check(lib().pb2_plan_tree_subbands(h, i, flo, fhi, info.nsubbands))
+            tree.n_to_flo, tree.n_to_fhi = list(flo), list(fhi)
+            self.trees.append(tree)
         d = config.to_dict()
         self.dtype = d["dtype"]
         self.nfreq = config.get_total_nfreq()
@@ -262,6 +281,25 @@ class DedispersionPlan:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.pb2_plan_destroy(self._h)
             self._h = None
+
+
+class PfAvarApproximation:
+    """pirate's PfAvarApproximation (include/pirate/PfVariance.hpp:86-120): analytic variances of the
+    peak finder's trials under unit weights, for white-noise input with per-channel variances
+    freq_variances (length nfreq, all > 0). tree_variance[itree] has shape (N, ndm_wt, nprofiles)."""
+
+    def __init__(self, plan, freq_variances):
+        fv = np.ascontiguousarray(freq_variances, dtype=np.float64)
+        if fv.ndim != 1:
+            raise RuntimeError("PfAvarApproximation: freq_variances must be one-dimensional")
+        self.nfreq = plan.nfreq
+        self.ntrees = plan.ntrees
+        self.tree_variance = [np.zeros((t.nsubbands, t.ndm_wt, t.nprofiles), dtype=np.float64) for t in plan.trees]
+        ptrs = (ctypes.POINTER(ctypes.c_double) * self.ntrees)(
+            *[a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for a in self.tree_variance])
+        lens = (ctypes.c_long * self.ntrees)(*[a.size for a in self.tree_variance])
+        _check(lib().pb2_plan_pf_variances(plan._h, fv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), fv.size,
+                                           ptrs, lens, self.ntrees))
 
 
 _TORCH_DTYPES = {0: "float32", 1: "float16", 2: "bfloat16"}
@@ -390,6 +428,15 @@ class GpuDedisperser:
         """pf_weights: (nbatches_wt, beams_per_batch, ndm_wt, nt_wt, nprofiles, N) float32."""
         w = np.ascontiguousarray(pf_weights, dtype=np.float32)
         _check(lib().pb2_dd_fill_weights(self._h, int(itree), w.ctypes.data, w.size))
+
+    def fill_analytic_weights(self, freq_variances):
+        """Every weight slot and beam gets the analytic SNR weights 1/sqrt(variance) of
+        PfAvarApproximation(plan, freq_variances) (src_lib/GpuDedisperser.cpp:1162-1238). Blocks until
+        the weights are on the GPU."""
+        fv = np.ascontiguousarray(freq_variances, dtype=np.float64)
+        if fv.ndim != 1:
+            raise RuntimeError("fill_analytic_weights: freq_variances must be one-dimensional")
+        _check(lib().pb2_dd_fill_analytic_weights(self._h, fv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), fv.size))
 
     def stop(self):
         _check(lib().pb2_dd_stop(self._h))

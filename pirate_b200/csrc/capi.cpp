@@ -3,6 +3,7 @@
 #include "../../include/pirate_b200.h"
 #include "dedisperser.hpp"
 #include "plan.hpp"
+#include "avar.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -108,6 +109,40 @@ int pb2_plan_to_yaml(const pb2_plan *plan, char *buf, long buflen, long *needed)
 int pb2_plan_ntrees(const pb2_plan *plan, long *ntrees)
 {
     return guard([&] { REQUIRE_PTR(plan); REQUIRE_PTR(ntrees); *ntrees = plan->p->ntrees; });
+}
+
+int pb2_plan_tree_subbands(const pb2_plan *plan, long itree, long *n_to_flo, long *n_to_fhi, long n)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(n_to_flo); REQUIRE_PTR(n_to_fhi);
+        if (itree < 0 || itree >= plan->p->ntrees) throw std::runtime_error("pb2_plan_tree_subbands: itree out of range");
+        const FrequencySubbands &fs = plan->p->trees[itree].frequency_subbands;
+        if (n != fs.N) throw std::runtime_error("pb2_plan_tree_subbands: n must equal the tree's number of subbands N");
+        for (long i = 0; i < n; i++) {
+            n_to_flo[i] = fs.n_to_flo[i];
+            n_to_fhi[i] = fs.n_to_fhi[i];
+        }
+    });
+}
+
+int pb2_plan_pf_variances(const pb2_plan *plan, const double *freq_variances, long nfreq, double *const *out,
+                          const long *out_len, long ntrees)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(freq_variances); REQUIRE_PTR(out); REQUIRE_PTR(out_len);
+        const DedispersionPlan &p = *plan->p;
+        if (ntrees != p.ntrees) throw std::runtime_error("pb2_plan_pf_variances: ntrees must equal the plan's number of trees");
+        for (long t = 0; t < ntrees; t++) {
+            const DedispersionTree &tr = p.trees[t];
+            const long want = tr.frequency_subbands.N * tr.ndm_wt * tr.nprofiles;
+            if (!out[t] || out_len[t] != want)
+                throw std::runtime_error("pb2_plan_pf_variances: out[" + std::to_string(t) + "] must hold N * ndm_wt * nprofiles = "
+                                         + std::to_string(want) + " doubles");
+        }
+        std::vector<std::vector<double>> v = pf_analytic_variances(p, freq_variances, nfreq);
+        for (long t = 0; t < ntrees; t++)
+            std::copy(v[t].begin(), v[t].end(), out[t]);
+    });
 }
 
 int pb2_plan_tree_info(const pb2_plan *plan, long itree, pb2_tree_info *o)
@@ -270,6 +305,11 @@ int pb2_dd_release_output(pb2_dedisperser *dd, long consumer_id, long seq_id, vo
 int pb2_dd_fill_weights(pb2_dedisperser *dd, long itree, const float *host, long nelts)
 {
     return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(host); dd->d->fill_all_weights(itree, host, nelts); });
+}
+
+int pb2_dd_fill_analytic_weights(pb2_dedisperser *dd, const double *freq_variances, long nfreq)
+{
+    return guard([&] { REQUIRE_PTR(dd); dd->d->fill_analytic_weights(freq_variances, nfreq); });
 }
 
 int pb2_dd_stop(pb2_dedisperser *dd)

@@ -1,6 +1,7 @@
 // dedisperser.cu -- host driver of the B200 dedispersion path (see dedisperser.hpp).
 
 #include "dedisperser.hpp"
+#include "avar.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -549,6 +550,24 @@ void GpuDedisperser::fill_all_weights(long itree, const float *host, long nelts)
                                 "(nbatches_wt, beams_per_batch, ndm_wt, nt_wt, nprofiles, N), got " + std::to_string(nelts));
         CUDA_CHECK(cudaMemcpyAsync(s2[itree].wt.ptr, host, nelts * sizeof(float), cudaMemcpyHostToDevice, compute));
         CUDA_CHECK(cudaStreamSynchronize(compute));
+    });
+}
+
+// GpuDedisperser::fill_analytic_weights (src_lib/GpuDedisperser.cpp:1162-1238): one beam's weights
+// per tree from the analytic variances, copied to every (weight batch, beam) slot on the compute stream.
+void GpuDedisperser::fill_analytic_weights(const double *freq_variances, long nfreq)
+{
+    entry([&]() {
+        if (!allocated) throw runtime_error("GpuDedisperser::fill_analytic_weights(): allocate() was not called");
+        std::vector<std::vector<double>> var = pf_analytic_variances(plan, freq_variances, nfreq);
+        for (long itree = 0; itree < plan.ntrees; itree++) {
+            std::vector<float> w = pf_weights_from_variances(plan.trees[itree], var[itree]);
+            const size_t nb = w.size() * sizeof(float);
+            char *dst = (char *) s2[itree].wt.ptr;
+            for (long slot = 0; slot < nbatches_wt * B; slot++)
+                CUDA_CHECK(cudaMemcpyAsync(dst + slot * nb, w.data(), nb, cudaMemcpyHostToDevice, compute));
+            CUDA_CHECK(cudaStreamSynchronize(compute));
+        }
     });
 }
 

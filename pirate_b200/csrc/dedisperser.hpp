@@ -79,6 +79,9 @@ public:
     Outputs acquire_output(long consumer_id, long seq_id, cudaStream_t stream, bool sync);
     void release_output(long consumer_id, long seq_id, cudaStream_t stream);
     void fill_all_weights(long itree, const float *host, long nelts);
+    // Fills every weight slot and beam of every tree with the analytic SNR weights made from the
+    // per-channel input variances (nfreq values > 0), and waits until they are on the GPU.
+    void fill_analytic_weights(const double *freq_variances, long nfreq);
     void stop(std::exception_ptr e = nullptr);
 
     // Device bytes held by allocate() (for reporting).
