@@ -82,6 +82,15 @@ int pb2_plan_stage1_ranks(const pb2_plan *plan, long *dd_rank, long *amb_rank, l
 int pb2_plan_decode_argmax(const pb2_plan *plan, uint32_t token, long itree, long idm, long itime, long *out5);
 /* DedispersionPlan::decode_argmax2, src_lib/DedispersionPlan.cpp:544; out5 = (freq_lo, freq_hi, dm, time, width) */
 int pb2_plan_decode_argmax2(const pb2_plan *plan, long itree, const long *in5, double *out5);
+/* DedispersionPlan.decode_argmax_batch / decode_argmax2_batch (src_pybind11/pirate_pybind11.cpp:396-409):
+ * decode_argmax / decode_argmax2 over n >= 1 events, element by element (the first bad element fails
+ * the call). Host arrays of length n. */
+int pb2_plan_decode_argmax_batch(const pb2_plan *plan, long n, const uint32_t *tokens, const long *itrees,
+                                 const long *idms, const long *itimes, long *fmins, long *fmaxs, long *tlos,
+                                 long *this_, long *ps);
+int pb2_plan_decode_argmax2_batch(const pb2_plan *plan, long n, const long *itrees, const long *fmins,
+                                  const long *fmaxs, const long *tlos, const long *this_, const long *ps,
+                                  double *freqs_lo, double *freqs_hi, double *dms, double *times, double *widths);
 /* DedispersionPlan::compute_steady_state_it0, src_lib/DedispersionPlan.cpp:634; out has ndm_out entries */
 int pb2_plan_steady_state_it0(const pb2_plan *plan, long itree, long *out, long n);
 
@@ -106,6 +115,15 @@ typedef struct pb2_outputs {
     void *out_max[PB2_MAX_TREES];
     uint32_t *out_argmax[PB2_MAX_TREES];
 } pb2_outputs;
+
+/* The toy grouper's per-chunk reduction (pirate_frb/run_toy_grouper.py:79-116), as one kernel on
+ * 'stream' over an acquired batch of outputs: per beam b < outs->nbeams, the largest out_max over
+ * every tree, dm and time (a tree whose maximum is NaN is passed over; ties go to the first tree, then
+ * the first (dm, time) in row-major order), with its tree, dm and time indices and the out_argmax
+ * token there. Device arrays of outs->nbeams entries; peak = -inf and tree = idm = itime = -1 when no
+ * tree qualifies. Call it while the outputs are acquired. */
+int pb2_beam_peaks(const pb2_outputs *outs, float *peak, int32_t *tree, int32_t *idm, int32_t *itime, uint32_t *token,
+                   void *stream);
 
 /* GpuDedisperser::create(params), src_lib/GpuDedisperser.cpp:84 */
 int pb2_dd_create(const pb2_plan *plan, const pb2_dd_params *params, pb2_dedisperser **out);

@@ -841,11 +841,24 @@ struct Dedisperser
             throw runtime_error("oracle: sophistication must be 0 or 1");
     }
 
-    // in: (B, F, nt_in) float; wts[itree]: (B, ndm_wt, nt_wt, P, N); outputs (B, ndm_out, nt_out).
-    void dedisperse(long ibatch, const float *in, const float *const *wts, R *const *omax, uint32_t *const *oarg)
+    // Tree-domain input (ReferenceDedisperser with tree_domain_input, src_lib/ReferenceDedisperser.cpp:205-213,
+    // 388-396): 'in' is already gridded, (B, 2^rtop, nt_in), and step 0 is a copy.
+    void load_tree_domain(R *dst, const float *in) const
+    {
+        for (long i = 0; i < B * pow2(rtop) * nt_in; i++)
+            dst[i] = R(in[i]);
+    }
+
+    // in: (B, F, nt_in) float, or (B, 2^rtop, nt_in) with tree_domain; wts[itree]: (B, ndm_wt, nt_wt, P, N);
+    // outputs (B, ndm_out, nt_out).
+    void dedisperse(long ibatch, const float *in, const float *const *wts, R *const *omax, uint32_t *const *oarg,
+                    bool tree_domain = false)
     {
         if (sophistication == 0) {
-            grid->apply(ds_inputs[0].data(), in, B);
+            if (tree_domain)
+                load_tree_domain(ds_inputs[0].data(), in);
+            else
+                grid->apply(ds_inputs[0].data(), in, B);
             for (long ip = 1; ip < npri; ip++) {
                 const R w = R(0.7071067811865476);
                 long ntd = xdiv(nt_in, pow2(ip));
@@ -876,7 +889,10 @@ struct Dedisperser
             return;
         }
 
-        grid->apply(s1buf[0].data(), in, B);
+        if (tree_domain)
+            load_tree_domain(s1buf[0].data(), in);
+        else
+            grid->apply(s1buf[0].data(), in, B);
         vector<R *> louts;
         for (long ip = 1; ip < npri; ip++) louts.push_back(s1buf[ip].data());
         lds->apply(s1buf[0].data(), louts.data(), ibatch);
@@ -1188,15 +1204,16 @@ int orc_channel_map(void *hv, double *out)
     return 0;
 }
 
-// Outputs are written as double regardless of the oracle's arithmetic type.
+// Outputs are written as double regardless of the oracle's arithmetic type. tree_domain != 0: 'in' is
+// tree-domain input (B, 2^toplevel_tree_rank, nt_in) instead of (B, nfreq, nt_in).
 int orc_dedisperse(void *hv, long ibatch, const float *in, const float *const *wts, double *const *omax,
-                   uint32_t *const *oarg)
+                   uint32_t *const *oarg, int tree_domain)
 {
     try {
         orc_handle *h = (orc_handle *) hv;
         long nt = h->plan->trees.size();
         if (h->real_bits == 64) {
-            h->d64->dedisperse(ibatch, in, wts, omax, oarg);
+            h->d64->dedisperse(ibatch, in, wts, omax, oarg, tree_domain != 0);
             return 0;
         }
         vector<vector<float>> tmp(nt);
@@ -1206,7 +1223,7 @@ int orc_dedisperse(void *hv, long ibatch, const float *in, const float *const *w
             tmp[i].resize(h->plan->config.beams_per_batch * t.ndm_out * t.nt_out);
             ptrs[i] = tmp[i].data();
         }
-        h->d32->dedisperse(ibatch, in, wts, ptrs.data(), oarg);
+        h->d32->dedisperse(ibatch, in, wts, ptrs.data(), oarg, tree_domain != 0);
         for (long i = 0; i < nt; i++)
             for (size_t k = 0; k < tmp[i].size(); k++)
                 omax[i][k] = tmp[i][k];

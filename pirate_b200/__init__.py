@@ -14,8 +14,8 @@ import os
 
 import numpy as np
 
-__all__ = ["DedispersionConfig", "DedispersionPlan", "GpuDedisperser", "Outputs", "PfAvarApproximation", "dequantize",
-           "lib", "LIB_PATH"]
+__all__ = ["DedispersionConfig", "DedispersionPlan", "GpuDedisperser", "Outputs", "PfAvarApproximation", "beam_peaks",
+           "dequantize", "lib", "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 # The in-tree build; PB2_LIBRARY names another build of the same library (for example one made with
@@ -77,6 +77,9 @@ def lib():
         "pb2_plan_decode_argmax": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_long, ctypes.c_long, ctypes.c_long, lp]),
         "pb2_plan_decode_argmax2": (ctypes.c_int, [vp, ctypes.c_long, lp, dp]),
         "pb2_plan_steady_state_it0": (ctypes.c_int, [vp, ctypes.c_long, lp, ctypes.c_long]),
+        "pb2_plan_decode_argmax_batch": (ctypes.c_int, [vp, ctypes.c_long, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "pb2_plan_decode_argmax2_batch": (ctypes.c_int, [vp, ctypes.c_long, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "pb2_beam_peaks": (ctypes.c_int, [ctypes.POINTER(_Outputs), vp, vp, vp, vp, vp, vp]),
         "pb2_plan_tree_subbands": (ctypes.c_int, [vp, ctypes.c_long, lp, lp, ctypes.c_long]),
         "pb2_plan_pf_variances": (ctypes.c_int, [vp, dp, ctypes.c_long, ctypes.POINTER(dp), lp, ctypes.c_long]),
         "pb2_dd_fill_analytic_weights": (ctypes.c_int, [vp, dp, ctypes.c_long]),
@@ -271,6 +274,32 @@ class DedispersionPlan:
         _check(lib().pb2_plan_decode_argmax2(self._h, int(itree), inp, out))
         return tuple(out)
 
+    def decode_argmax_batch(self, tokens, itrees, idms, itimes):
+        """Vectorized decode_argmax over nonempty 1-d arrays (one event per element). Returns
+        (fmins, fmaxs, tlos, this, ps), int64 arrays (src_pybind11/pirate_pybind11.cpp:396-401)."""
+        tok = np.ascontiguousarray(tokens, dtype=np.uint32)
+        its, ids, itm = (np.ascontiguousarray(a, dtype=np.int64) for a in (itrees, idms, itimes))
+        n = tok.size
+        if tok.ndim != 1 or any(a.shape != tok.shape for a in (its, ids, itm)):
+            raise RuntimeError("decode_argmax_batch: tokens, itrees, idms and itimes must be 1-d of one length")
+        outs = [np.zeros(n, dtype=np.int64) for _ in range(5)]
+        _check(lib().pb2_plan_decode_argmax_batch(self._h, n, tok.ctypes.data, its.ctypes.data, ids.ctypes.data,
+                                                  itm.ctypes.data, *[o.ctypes.data for o in outs]))
+        return tuple(outs)
+
+    def decode_argmax2_batch(self, itrees, fmins, fmaxs, tlos, this, ps):
+        """Vectorized decode_argmax2: (freqs_lo_MHz, freqs_hi_MHz, dms, timestamps_samp, widths_samp),
+        float64 arrays; timestamps are chunk-relative toplevel samples
+        (src_pybind11/pirate_pybind11.cpp:402-409)."""
+        ins = [np.ascontiguousarray(a, dtype=np.int64) for a in (itrees, fmins, fmaxs, tlos, this, ps)]
+        n = ins[0].size
+        if ins[0].ndim != 1 or any(a.shape != ins[0].shape for a in ins):
+            raise RuntimeError("decode_argmax2_batch: the arrays must be 1-d of one length")
+        outs = [np.zeros(n, dtype=np.float64) for _ in range(5)]
+        _check(lib().pb2_plan_decode_argmax2_batch(self._h, n, *[a.ctypes.data for a in ins],
+                                                   *[o.ctypes.data for o in outs]))
+        return tuple(outs)
+
     def compute_steady_state_it0(self, itree):
         n = self.trees[itree].ndm_out
         out = np.zeros(n, dtype=np.int64)
@@ -324,6 +353,7 @@ class Outputs:
     """GpuDedisperser::Outputs (include/pirate/Dedisperser.hpp:98-125); arrays are torch views."""
 
     def __init__(self, o, device):
+        self._raw = o
         self.dtype = _TORCH_DTYPES[o.dtype]
         self.nbeams = o.nbeams
         self.ichunk_zero_based = o.ichunk_zero_based
@@ -474,6 +504,46 @@ class GpuDedisperser:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.pb2_dd_destroy(self._h)
             self._h = None
+
+
+def beam_peaks(outputs, stream=None, out=None):
+    """The toy grouper's per-chunk reduction of one batch of outputs (pirate_frb/run_toy_grouper.py:
+    79-116), in one kernel: per beam, the largest out_max over all trees, dm and time, its tree, dm and
+    time indices and the out_argmax token there (a tree whose maximum is NaN is passed over; ties go to
+    the first tree, then the first (dm, time)). 'outputs' is an acquired Outputs, or a pair of lists
+    (out_max, out_argmax) of device tensors shaped (nbeams, ndm_out, nt_out). 'out', if given, is
+    (peak float32, tree int32, idm int32, itime int32, token int32 view of uint32), each of nbeams
+    entries; otherwise new tensors are returned in that order."""
+    import torch
+    if isinstance(outputs, Outputs):
+        raw = outputs._raw
+        nbeams = outputs.nbeams
+        device = outputs.out_max[0].device
+    else:
+        maxes, args = outputs
+        codes = {torch.float32: 0, torch.float16: 1, torch.bfloat16: 2}
+        if not maxes or len(maxes) != len(args) or len(maxes) > MAX_TREES:
+            raise RuntimeError("beam_peaks: need 1..%d (out_max, out_argmax) pairs" % MAX_TREES)
+        raw = _Outputs()
+        raw.dtype = codes[maxes[0].dtype]
+        raw.nbeams = maxes[0].shape[0]
+        raw.ntrees = len(maxes)
+        for i, (m, a) in enumerate(zip(maxes, args)):
+            if m.dtype != maxes[0].dtype or not m.is_contiguous() or not a.is_contiguous() or m.dim() != 3 \
+                    or tuple(a.shape) != tuple(m.shape) or a.element_size() != 4 or m.shape[0] != raw.nbeams:
+                raise RuntimeError("beam_peaks: arrays must be contiguous (nbeams, ndm_out, nt_out), one dtype")
+            raw.ndm_out[i], raw.nt_out[i] = m.shape[1], m.shape[2]
+            raw.out_max[i], raw.out_argmax[i] = m.data_ptr(), a.data_ptr()
+        nbeams = raw.nbeams
+        device = maxes[0].device
+    if out is None:
+        out = (torch.empty(nbeams, dtype=torch.float32, device=device),
+               *[torch.empty(nbeams, dtype=torch.int32, device=device) for _ in range(4)])
+    for t, dt in zip(out, (torch.float32, torch.int32, torch.int32, torch.int32, torch.int32)):
+        if t.dtype != dt or t.numel() != nbeams or not t.is_contiguous():
+            raise RuntimeError("beam_peaks: out must be (float32, int32 x 4) tensors of nbeams entries")
+    _check(lib().pb2_beam_peaks(ctypes.byref(raw), *[t.data_ptr() for t in out], _stream_ptr(stream)))
+    return out
 
 
 def dequantize(out, scales_offsets, data, stream=None):

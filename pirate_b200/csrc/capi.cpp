@@ -4,6 +4,7 @@
 #include "dedisperser.hpp"
 #include "plan.hpp"
 #include "avar.hpp"
+#include "kernels.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -195,6 +196,54 @@ int pb2_plan_decode_argmax2(const pb2_plan *plan, long itree, const long *in5, d
     return guard([&] {
         REQUIRE_PTR(plan); REQUIRE_PTR(in5); REQUIRE_PTR(o);
         plan->p->decode_argmax2(itree, in5[0], in5[1], in5[2], in5[3], in5[4], o[0], o[1], o[2], o[3], o[4]);
+    });
+}
+
+int pb2_plan_decode_argmax_batch(const pb2_plan *plan, long n, const uint32_t *tokens, const long *itrees,
+                                 const long *idms, const long *itimes, long *fmins, long *fmaxs, long *tlos,
+                                 long *this_, long *ps)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(tokens); REQUIRE_PTR(itrees); REQUIRE_PTR(idms); REQUIRE_PTR(itimes);
+        REQUIRE_PTR(fmins); REQUIRE_PTR(fmaxs); REQUIRE_PTR(tlos); REQUIRE_PTR(this_); REQUIRE_PTR(ps);
+        if (n <= 0) throw std::runtime_error("decode_argmax_batch: the arrays must be nonempty");
+        for (long i = 0; i < n; i++)
+            plan->p->decode_argmax(tokens[i], itrees[i], idms[i], itimes[i], fmins[i], fmaxs[i], tlos[i], this_[i], ps[i]);
+    });
+}
+
+int pb2_plan_decode_argmax2_batch(const pb2_plan *plan, long n, const long *itrees, const long *fmins,
+                                  const long *fmaxs, const long *tlos, const long *this_, const long *ps,
+                                  double *freqs_lo, double *freqs_hi, double *dms, double *times, double *widths)
+{
+    return guard([&] {
+        REQUIRE_PTR(plan); REQUIRE_PTR(itrees); REQUIRE_PTR(fmins); REQUIRE_PTR(fmaxs); REQUIRE_PTR(tlos);
+        REQUIRE_PTR(this_); REQUIRE_PTR(ps); REQUIRE_PTR(freqs_lo); REQUIRE_PTR(freqs_hi); REQUIRE_PTR(dms);
+        REQUIRE_PTR(times); REQUIRE_PTR(widths);
+        if (n <= 0) throw std::runtime_error("decode_argmax2_batch: the arrays must be nonempty");
+        for (long i = 0; i < n; i++)
+            plan->p->decode_argmax2(itrees[i], fmins[i], fmaxs[i], tlos[i], this_[i], ps[i], freqs_lo[i], freqs_hi[i],
+                                    dms[i], times[i], widths[i]);
+    });
+}
+
+int pb2_beam_peaks(const pb2_outputs *outs, float *peak, int32_t *tree, int32_t *idm, int32_t *itime, uint32_t *token,
+                   void *stream)
+{
+    return guard([&] {
+        REQUIRE_PTR(outs); REQUIRE_PTR(peak); REQUIRE_PTR(tree); REQUIRE_PTR(idm); REQUIRE_PTR(itime); REQUIRE_PTR(token);
+        if (outs->ntrees < 1 || outs->ntrees > PB2_MAX_TREES) throw std::runtime_error("pb2_beam_peaks: bad ntrees");
+        pb2::BeamPeakArgs a;
+        memset(&a, 0, sizeof(a));
+        a.ntrees = int(outs->ntrees);
+        for (long t = 0; t < outs->ntrees; t++) {
+            a.ndm[t] = outs->ndm_out[t];
+            a.nt[t] = outs->nt_out[t];
+            a.out_max[t] = outs->out_max[t];
+            a.out_argmax[t] = outs->out_argmax[t];
+        }
+        a.peak = peak; a.tree = tree; a.idm = idm; a.itime = itime; a.token = token;
+        pb2::launch_beam_peaks(a, outs->dtype, outs->nbeams, (cudaStream_t) stream);
     });
 }
 

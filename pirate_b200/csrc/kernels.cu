@@ -219,6 +219,151 @@ void launch_dequantize(void *out, int out_dtype, const void *data, const void *s
     check_launch("dequant_kernel");
 }
 
+// ---------------------------------------------------------------------------------------------
+// Per-beam peak over a batch's outputs (the toy grouper's reduction, see BeamPeakArgs).
+// One 1024-thread block per beam scans every tree of that beam with 16-byte loads where the beam's
+// slice is aligned, keeping per thread the largest value and its first index; the block then
+// reduces with ties going to the smaller index, and thread 0 merges the trees in order.
+
+// 16 bytes of out_max as raw words; element k of them as fp32.
+template<typename T> struct PeakVec;
+template<> struct PeakVec<float>
+{
+    static constexpr int N = 4;
+    __device__ static float get(const uint4 &q, int k)
+    {
+        return __uint_as_float(k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w);
+    }
+};
+template<> struct PeakVec<__half>
+{
+    static constexpr int N = 8;
+    __device__ static float get(const uint4 &q, int k)
+    {
+        const uint32_t w = (k < 2) ? q.x : (k < 4) ? q.y : (k < 6) ? q.z : q.w;
+        return __half2float(__ushort_as_half((unsigned short) ((k & 1) ? (w >> 16) : (w & 0xffff))));
+    }
+};
+template<> struct PeakVec<__nv_bfloat16>
+{
+    static constexpr int N = 8;
+    __device__ static float get(const uint4 &q, int k)
+    {
+        const uint32_t w = (k < 2) ? q.x : (k < 4) ? q.y : (k < 6) ? q.z : q.w;
+        return __uint_as_float((k & 1) ? (w & 0xffff0000u) : (w << 16));
+    }
+};
+
+__device__ __forceinline__ void peak_take(float v, long i, float &bv, long &bi)
+{
+    if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
+}
+
+template<typename T>
+__global__ void __launch_bounds__(1024) beam_peak_kernel(BeamPeakArgs a)
+{
+    constexpr int V = PeakVec<T>::N;
+    constexpr long kNone = 0x7fffffffffffffffL;
+    __shared__ float rv[32];
+    __shared__ long ri[32];
+    __shared__ int rn[32];
+    const int b = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+
+    float gv = -INFINITY;            // thread 0: best over the trees so far
+    int gt = -1;
+    long gi = 0;
+
+    for (int t = 0; t < a.ntrees; t++) {
+        const long n = a.ndm[t] * a.nt[t];
+        const T *x = (const T *) a.out_max[t] + (long) b * n;
+        float bv = -INFINITY;
+        long bi = kNone;
+        bool nan = false;
+        if (n % V == 0 && ((uintptr_t) x & 15) == 0) {
+            const long nv = n / V;
+            const uint4 *xv = (const uint4 *) x;
+            for (long j = threadIdx.x; j < nv; j += 4L * blockDim.x) {
+                uint4 q[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const long jj = j + (long) u * blockDim.x;
+                    if (jj < nv) q[u] = __ldg(xv + jj);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const long jj = j + (long) u * blockDim.x;
+                    if (jj < nv) {
+#pragma unroll
+                        for (int k = 0; k < V; k++) {
+                            const float v = PeakVec<T>::get(q[u], k);
+                            nan |= (v != v);
+                            if (v > bv) { bv = v; bi = jj * V + k; }
+                        }
+                    }
+                }
+            }
+        } else {
+            for (long i = threadIdx.x; i < n; i += blockDim.x) {
+                const float v = to_f(x[i]);
+                nan |= (v != v);
+                if (v > bv) { bv = v; bi = i; }
+            }
+        }
+
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            peak_take(__shfl_down_sync(0xffffffffu, bv, o), __shfl_down_sync(0xffffffffu, bi, o), bv, bi);
+        const bool wnan = __any_sync(0xffffffffu, nan);
+        if (lane == 0) { rv[warp] = bv; ri[warp] = bi; rn[warp] = wnan; }
+        __syncthreads();
+        if (warp == 0) {
+            bv = (lane < nwarps) ? rv[lane] : -INFINITY;
+            bi = (lane < nwarps) ? ri[lane] : kNone;
+            const bool tnan = __any_sync(0xffffffffu, (lane < nwarps) && rn[lane]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                peak_take(__shfl_down_sync(0xffffffffu, bv, o), __shfl_down_sync(0xffffffffu, bi, o), bv, bi);
+            if (lane == 0 && !tnan && bv > gv) { gv = bv; gt = t; gi = bi; }
+        }
+        __syncthreads();
+    }
+
+    if (threadIdx.x == 0) {
+        a.peak[b] = gv;
+        a.tree[b] = gt;
+        if (gt >= 0) {
+            const long nt = a.nt[gt];
+            a.idm[b] = int(gi / nt);
+            a.itime[b] = int(gi % nt);
+            a.token[b] = a.out_argmax[gt][(long) b * a.ndm[gt] * nt + gi];
+        } else {
+            a.idm[b] = -1;
+            a.itime[b] = -1;
+            a.token[b] = 0;
+        }
+    }
+}
+
+void launch_beam_peaks(const BeamPeakArgs &a, int dtype, long nbeams, cudaStream_t s)
+{
+    if (a.ntrees < 0 || a.ntrees > kBeamPeakMaxTrees) throw std::runtime_error("beam_peaks: bad number of trees");
+    if (!a.peak || !a.tree || !a.idm || !a.itime || !a.token) throw std::runtime_error("beam_peaks: null output pointer");
+    for (int t = 0; t < a.ntrees; t++) {
+        if (!a.out_max[t] || !a.out_argmax[t]) throw std::runtime_error("beam_peaks: null output array");
+        if (a.ndm[t] <= 0 || a.nt[t] <= 0 || a.ndm[t] * a.nt[t] >= (1L << 31))
+            throw std::runtime_error("beam_peaks: tree shape out of range");
+    }
+    if (nbeams <= 0) return;
+    if (nbeams > 0x7fffffffL) throw std::runtime_error("beam_peaks: too many beams");
+    const unsigned grid = (unsigned) nbeams;
+    if (dtype == 0) beam_peak_kernel<float><<<grid, 1024, 0, s>>>(a);
+    else if (dtype == 1) beam_peak_kernel<__half><<<grid, 1024, 0, s>>>(a);
+    else if (dtype == 2) beam_peak_kernel<__nv_bfloat16><<<grid, 1024, 0, s>>>(a);
+    else throw std::runtime_error("beam_peaks: dtype must be 0 (float32), 1 (float16) or 2 (bfloat16)");
+    check_launch("beam_peak_kernel");
+}
+
 constexpr int kGridMaxThreads = 512;
 
 template<typename Ts, int NLEV, bool Q>

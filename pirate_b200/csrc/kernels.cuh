@@ -119,6 +119,23 @@ struct GridLdsArgs
 inline long stage1_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), false); }
 inline long stage2_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), true); }
 
+// Per-beam peak of a batch's outputs, as pirate's toy grouper reduces them (pirate_frb/run_toy_grouper.py:
+// 79-116): over every tree, the maximum of out_max[tree][b] and its first (dm, time) position; a tree
+// whose maximum is NaN is passed over; across trees the first tree with the strictly largest maximum
+// wins. peak/tree/idm/itime/token hold nbeams entries (peak -inf and tree -1 when no tree qualified).
+constexpr int kBeamPeakMaxTrees = 64;
+struct BeamPeakArgs
+{
+    int ntrees;
+    long ndm[kBeamPeakMaxTrees], nt[kBeamPeakMaxTrees];
+    const void *out_max[kBeamPeakMaxTrees];
+    const uint32_t *out_argmax[kBeamPeakMaxTrees];
+    float *peak;
+    int *tree, *idm, *itime;
+    uint32_t *token;
+};
+void launch_beam_peaks(const BeamPeakArgs &a, int dtype, long nbeams, cudaStream_t s);
+
 void launch_grid_lds(const GridLdsArgs &a, int dtype, cudaStream_t s);
 // int4 -> out_dtype dequantization of (nbeams, nfreq, ntime) samples (ntime a multiple of 256).
 void launch_dequantize(void *out, int out_dtype, const void *data, const void *scales_offsets, long nbeams, long nfreq,

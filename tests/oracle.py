@@ -46,7 +46,7 @@ def lib():
         L.orc_channel_map.argtypes = [ctypes.c_void_p, c_double_p]
         L.orc_dedisperse.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
                                      ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
-                                     ctypes.POINTER(ctypes.c_void_p)]
+                                     ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
         L.orc_eval_tokens.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p]
         L.orc_gridded.argtypes = [ctypes.c_void_p, c_double_p]
@@ -131,11 +131,12 @@ class OracleDedisperser:
         t = self.trees[i]
         return (self.B, t["ndm_out"], t["nt_out"])
 
-    def dedisperse(self, ibatch, x, weights):
-        """x: float32 (B, nfreq, nt_in); weights: list of float32 arrays of wt_shape(i).
-        Returns (out_max list (float64), out_argmax list (uint32))."""
+    def dedisperse(self, ibatch, x, weights, tree_domain=False):
+        """x: float32 (B, nfreq, nt_in), or with tree_domain (B, 2^toplevel_tree_rank, nt_in) already
+        gridded (ReferenceDedisperser's tree_domain_input); weights: list of float32 arrays of
+        wt_shape(i). Returns (out_max list (float64), out_argmax list (uint32))."""
         x = np.ascontiguousarray(x, dtype=np.float32)
-        assert x.shape == (self.B, self.nfreq, self.nt_in)
+        assert x.shape == (self.B, (1 << self.rank) if tree_domain else self.nfreq, self.nt_in)
         wts = [np.ascontiguousarray(w, dtype=np.float32) for w in weights]
         omax = [np.zeros(self.out_shape(i), dtype=np.float64) for i in range(self.ntrees)]
         oarg = [np.zeros(self.out_shape(i), dtype=np.uint32) for i in range(self.ntrees)]
@@ -143,7 +144,7 @@ class OracleDedisperser:
         wp = (ctypes.c_void_p * n)(*[w.ctypes.data for w in wts])
         mp = (ctypes.c_void_p * n)(*[a.ctypes.data for a in omax])
         ap = (ctypes.c_void_p * n)(*[a.ctypes.data for a in oarg])
-        rc = lib().orc_dedisperse(self.h, int(ibatch), x.ctypes.data, wp, mp, ap)
+        rc = lib().orc_dedisperse(self.h, int(ibatch), x.ctypes.data, wp, mp, ap, int(bool(tree_domain)))
         if rc != 0:
             raise RuntimeError("oracle: " + _err())
         self._last_wts = wts
