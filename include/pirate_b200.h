@@ -125,6 +125,41 @@ typedef struct pb2_outputs {
 int pb2_beam_peaks(const pb2_outputs *outs, float *peak, int32_t *tree, int32_t *idm, int32_t *itime, uint32_t *token,
                    void *stream);
 
+/* Simulated FRB pulses: pirate::simpulse (include/pirate/simpulse.hpp:24-119, src_lib/simpulse.cpp).
+ * dispersion_delay / scattering_time in seconds (simpulse.hpp:27,31). */
+int pb2_dispersion_delay(double dm, double freq_mhz, double *seconds);
+int pb2_scattering_time(double sm, double freq_mhz, double *seconds);
+
+/* SinglePulse::Params (include/pirate/simpulse.hpp:42-66) without the two arrays, which are passed
+ * separately: freq_edges_mhz (nfreq + 1, increasing) and freq_variances (nfreq). */
+typedef struct pb2_pulse_params {
+    double dm, sm, intrinsic_width, spectral_index, undispersed_arrival_time_sec, time_sample_ms, snr;
+    double subband_freq_lo_mhz, subband_freq_hi_mhz;    /* pirate's defaults: 0 and 1e9 */
+    long internal_nt;                                   /* pirate's default: 1024 */
+} pb2_pulse_params;
+typedef struct pb2_pulse pb2_pulse;
+
+/* SinglePulse(params), src_lib/simpulse.cpp:131-320 */
+int pb2_pulse_create(const pb2_pulse_params *params, const double *freq_edges_mhz, const double *freq_variances,
+                     long nfreq, pb2_pulse **out);
+void pb2_pulse_destroy(pb2_pulse *pulse);
+/* SinglePulse::it_start, it_end and the number of stored samples (sum of freq_nt). */
+int pb2_pulse_range(const pb2_pulse *pulse, long *it_start, long *it_end, long *nsamples);
+/* SinglePulse::freq_it0, freq_nt, freq_sd_off (nfreq each) and sparse_data (nsamples), copied out. */
+int pb2_pulse_sparse(const pb2_pulse *pulse, long *freq_it0, long *freq_nt, long *freq_sd_off, float *sparse_data);
+/* SinglePulse::add_to_timestream(out, out_it0, weight), src_lib/simpulse.cpp:323-360: host float32
+ * array of nfreq rows (row_stride elements apart) spanning samples [out_it0, out_it0 + out_nt). */
+int pb2_pulse_add_to_timestream(const pb2_pulse *pulse, float *out, long nfreq, long out_nt, long row_stride,
+                                long out_it0, float weight);
+/* SinglePulse::shift_samples(delta_it), src_lib/simpulse.cpp:363-373 */
+int pb2_pulse_shift_samples(pb2_pulse *pulse, long delta_it);
+/* Injection on the GPU, one kernel on 'stream': adds weight * pulse to a device chunk of nfreq rows
+ * (row_stride elements apart, dtype 0/1/2 = float32/float16/bfloat16) holding samples
+ * [chunk_it0, chunk_it0 + nt); pulse samples outside the chunk are skipped (the analogue of pirate's
+ * inject_single_pulse clipping). Copies the pulse to the current device on first use. */
+int pb2_pulse_inject(pb2_pulse *pulse, void *chunk, int dtype, long nfreq, long nt, long row_stride, long chunk_it0,
+                     float weight, void *stream);
+
 /* GpuDedisperser::create(params), src_lib/GpuDedisperser.cpp:84 */
 int pb2_dd_create(const pb2_plan *plan, const pb2_dd_params *params, pb2_dedisperser **out);
 /* GpuDedisperser::allocate(gpu_allocator, host_allocator), src_lib/GpuDedisperser.cpp:390 (allocates internally) */

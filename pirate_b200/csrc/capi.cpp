@@ -5,6 +5,7 @@
 #include "plan.hpp"
 #include "avar.hpp"
 #include "kernels.cuh"
+#include "simpulse.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -17,6 +18,9 @@ using namespace pb2;
 struct pb2_config { DedispersionConfig c; };
 struct pb2_plan { std::shared_ptr<DedispersionPlan> p; };
 struct pb2_dedisperser { std::unique_ptr<GpuDedisperser> d; };
+
+#define CUDA_CHECK(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) \
+    throw std::runtime_error(std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
 
 static thread_local std::string g_err;
 
@@ -224,6 +228,112 @@ int pb2_plan_decode_argmax2_batch(const pb2_plan *plan, long n, const long *itre
         for (long i = 0; i < n; i++)
             plan->p->decode_argmax2(itrees[i], fmins[i], fmaxs[i], tlos[i], this_[i], ps[i], freqs_lo[i], freqs_hi[i],
                                     dms[i], times[i], widths[i]);
+    });
+}
+
+struct pb2_pulse
+{
+    std::unique_ptr<pb2::SinglePulse> p;
+    long *d_idx = nullptr;      // device copies for injection: it0, cnt, off (3 * nfreq)
+    float *d_data = nullptr;
+    int device = -1;
+    ~pb2_pulse()
+    {
+        if (d_idx) cudaFree(d_idx);
+        if (d_data) cudaFree(d_data);
+    }
+};
+
+int pb2_dispersion_delay(double dm, double freq_mhz, double *out)
+{
+    return guard([&] { REQUIRE_PTR(out); *out = pb2::dispersion_delay(dm, freq_mhz); });
+}
+
+int pb2_scattering_time(double sm, double freq_mhz, double *out)
+{
+    return guard([&] { REQUIRE_PTR(out); *out = pb2::scattering_time(sm, freq_mhz); });
+}
+
+int pb2_pulse_create(const pb2_pulse_params *pp, const double *freq_edges_mhz, const double *freq_variances, long nfreq,
+                     pb2_pulse **out)
+{
+    return guard([&] {
+        REQUIRE_PTR(pp); REQUIRE_PTR(freq_edges_mhz); REQUIRE_PTR(freq_variances); REQUIRE_PTR(out);
+        if (nfreq < 1) throw std::runtime_error("SinglePulse: nfreq must be >= 1");
+        pb2::SinglePulseParams p;
+        p.dm = pp->dm; p.sm = pp->sm; p.intrinsic_width = pp->intrinsic_width; p.spectral_index = pp->spectral_index;
+        p.undispersed_arrival_time_sec = pp->undispersed_arrival_time_sec; p.time_sample_ms = pp->time_sample_ms;
+        p.snr = pp->snr; p.subband_freq_lo_mhz = pp->subband_freq_lo_mhz; p.subband_freq_hi_mhz = pp->subband_freq_hi_mhz;
+        p.internal_nt = pp->internal_nt;
+        p.freq_edges_mhz.assign(freq_edges_mhz, freq_edges_mhz + nfreq + 1);
+        p.freq_variances.assign(freq_variances, freq_variances + nfreq);
+        std::unique_ptr<pb2_pulse> h(new pb2_pulse);
+        h->p.reset(new pb2::SinglePulse(p));
+        *out = h.release();
+    });
+}
+
+void pb2_pulse_destroy(pb2_pulse *pulse) { delete pulse; }
+
+int pb2_pulse_range(const pb2_pulse *pulse, long *it_start, long *it_end, long *nsamples)
+{
+    return guard([&] {
+        REQUIRE_PTR(pulse); REQUIRE_PTR(it_start); REQUIRE_PTR(it_end); REQUIRE_PTR(nsamples);
+        *it_start = pulse->p->it_start;
+        *it_end = pulse->p->it_end;
+        *nsamples = (long) pulse->p->sparse_data.size();
+    });
+}
+
+int pb2_pulse_sparse(const pb2_pulse *pulse, long *freq_it0, long *freq_nt, long *freq_sd_off, float *sparse_data)
+{
+    return guard([&] {
+        REQUIRE_PTR(pulse); REQUIRE_PTR(freq_it0); REQUIRE_PTR(freq_nt); REQUIRE_PTR(freq_sd_off); REQUIRE_PTR(sparse_data);
+        const pb2::SinglePulse &sp = *pulse->p;
+        std::copy(sp.freq_it0.begin(), sp.freq_it0.end(), freq_it0);
+        std::copy(sp.freq_nt.begin(), sp.freq_nt.end(), freq_nt);
+        std::copy(sp.freq_sd_off.begin(), sp.freq_sd_off.end(), freq_sd_off);
+        std::copy(sp.sparse_data.begin(), sp.sparse_data.end(), sparse_data);
+    });
+}
+
+int pb2_pulse_add_to_timestream(const pb2_pulse *pulse, float *out, long nfreq, long out_nt, long row_stride,
+                                long out_it0, float weight)
+{
+    return guard([&] { REQUIRE_PTR(pulse); pulse->p->add_to_timestream(out, nfreq, out_nt, row_stride, out_it0, weight); });
+}
+
+int pb2_pulse_shift_samples(pb2_pulse *pulse, long delta_it)
+{
+    return guard([&] { REQUIRE_PTR(pulse); pulse->p->shift_samples(delta_it); });
+}
+
+int pb2_pulse_inject(pb2_pulse *pulse, void *chunk, int dtype, long nfreq, long nt, long row_stride, long chunk_it0,
+                     float weight, void *stream)
+{
+    return guard([&] {
+        REQUIRE_PTR(pulse); REQUIRE_PTR(chunk);
+        const pb2::SinglePulse &sp = *pulse->p;
+        if (nfreq != sp.nfreq) throw std::runtime_error("pb2_pulse_inject: the chunk must have one row per pulse channel");
+        int dev = 0;
+        CUDA_CHECK(cudaGetDevice(&dev));
+        if (pulse->d_idx && pulse->device != dev) {
+            cudaFree(pulse->d_idx); cudaFree(pulse->d_data);
+            pulse->d_idx = nullptr; pulse->d_data = nullptr;
+        }
+        if (!pulse->d_idx) {
+            std::vector<long> idx(3 * sp.nfreq);
+            std::copy(sp.freq_it0.begin(), sp.freq_it0.end(), idx.begin());
+            std::copy(sp.freq_nt.begin(), sp.freq_nt.end(), idx.begin() + sp.nfreq);
+            std::copy(sp.freq_sd_off.begin(), sp.freq_sd_off.end(), idx.begin() + 2 * sp.nfreq);
+            CUDA_CHECK(cudaMalloc((void **) &pulse->d_idx, idx.size() * sizeof(long)));
+            CUDA_CHECK(cudaMalloc((void **) &pulse->d_data, sp.sparse_data.size() * sizeof(float)));
+            pulse->device = dev;
+            CUDA_CHECK(cudaMemcpy(pulse->d_idx, idx.data(), idx.size() * sizeof(long), cudaMemcpyHostToDevice));
+            CUDA_CHECK(cudaMemcpy(pulse->d_data, sp.sparse_data.data(), sp.sparse_data.size() * sizeof(float), cudaMemcpyHostToDevice));
+        }
+        pb2::launch_pulse_inject(chunk, dtype, nfreq, nt, row_stride, chunk_it0, pulse->d_idx, pulse->d_idx + sp.nfreq,
+                                 pulse->d_idx + 2 * sp.nfreq, pulse->d_data, weight, (cudaStream_t) stream);
     });
 }
 

@@ -364,6 +364,38 @@ void launch_beam_peaks(const BeamPeakArgs &a, int dtype, long nbeams, cudaStream
     check_launch("beam_peak_kernel");
 }
 
+// ---------------------------------------------------------------------------------------------
+// Pulse injection into a chunk (see launch_pulse_inject): one warp per channel, in the storage
+// dtype, as out = round(out + weight * value) with one fp32 multiply and one fp32 add.
+
+template<typename T>
+__global__ void pulse_inject_kernel(T *out, long nfreq, long nt, long row_stride, long chunk_it0, const long *it0,
+                                    const long *cnt, const long *off, const float *data, float weight)
+{
+    const long f = (long) blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (f >= nfreq) return;
+    const long a = it0[f] - chunk_it0;
+    const long jlo = (a < 0) ? -a : 0;
+    const long jhi = (cnt[f] < nt - a) ? cnt[f] : nt - a;
+    const float *src = data + off[f];
+    T *row = out + f * row_stride + a;
+    for (long j = jlo + (threadIdx.x & 31); j < jhi; j += 32)
+        row[j] = from_f<T>(__fadd_rn(to_f(row[j]), __fmul_rn(weight, src[j])));
+}
+
+void launch_pulse_inject(void *out, int dtype, long nfreq, long nt, long row_stride, long chunk_it0, const long *it0,
+                         const long *cnt, const long *off, const float *data, float weight, cudaStream_t s)
+{
+    if (!out || !it0 || !cnt || !off || !data) throw std::runtime_error("pulse_inject: null pointer");
+    if (nfreq <= 0 || nt <= 0 || row_stride < nt) throw std::runtime_error("pulse_inject: bad chunk shape");
+    const unsigned grid = (unsigned) ((nfreq + 7) / 8);
+    if (dtype == 0) pulse_inject_kernel<float><<<grid, 256, 0, s>>>((float *) out, nfreq, nt, row_stride, chunk_it0, it0, cnt, off, data, weight);
+    else if (dtype == 1) pulse_inject_kernel<__half><<<grid, 256, 0, s>>>((__half *) out, nfreq, nt, row_stride, chunk_it0, it0, cnt, off, data, weight);
+    else if (dtype == 2) pulse_inject_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>((__nv_bfloat16 *) out, nfreq, nt, row_stride, chunk_it0, it0, cnt, off, data, weight);
+    else throw std::runtime_error("pulse_inject: dtype must be 0 (float32), 1 (float16) or 2 (bfloat16)");
+    check_launch("pulse_inject_kernel");
+}
+
 constexpr int kGridMaxThreads = 512;
 
 template<typename Ts, int NLEV, bool Q>

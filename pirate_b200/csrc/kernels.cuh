@@ -136,6 +136,13 @@ struct BeamPeakArgs
 };
 void launch_beam_peaks(const BeamPeakArgs &a, int dtype, long nbeams, cudaStream_t s);
 
+// Adds a sparse pulse (channel f: cnt[f] samples from sample index it0[f], values data[off[f] ...])
+// times 'weight' to the chunk out (nfreq rows of row_stride elements, dtype 0/1/2 = f32/f16/bf16)
+// holding samples [chunk_it0, chunk_it0 + nt); samples outside the chunk are skipped. The index
+// arrays and data are device arrays.
+void launch_pulse_inject(void *out, int dtype, long nfreq, long nt, long row_stride, long chunk_it0, const long *it0,
+                         const long *cnt, const long *off, const float *data, float weight, cudaStream_t s);
+
 void launch_grid_lds(const GridLdsArgs &a, int dtype, cudaStream_t s);
 // int4 -> out_dtype dequantization of (nbeams, nfreq, ntime) samples (ntime a multiple of 256).
 void launch_dequantize(void *out, int out_dtype, const void *data, const void *scales_offsets, long nbeams, long nfreq,

@@ -261,3 +261,73 @@ def random_quantized(rng, nbeams, nfreq, ntime, missing=0.01):
     so[..., 0] = rng.uniform(0.0, 1.0, so.shape[:-1])
     so[..., 1] = rng.uniform(-1.0, 1.0, so.shape[:-1])
     return data, so
+
+
+# -------------------------------------------------------------------------------------------------
+# Simulated pulses: numpy restatement of pirate's SinglePulse constructor (src_lib/simpulse.cpp:131-320),
+# with numpy's FFT for the synthesis.
+
+K_DM = 4.148808e6            # ms MHz^2 per pc cm^-3 (include/pirate/constants.hpp:49)
+
+
+def single_pulse(dm, sm, intrinsic_width, spectral_index, undispersed_arrival_time_sec, time_sample_ms, snr,
+                 freq_edges_MHz, freq_variances, subband_freq_lo_MHz=0.0, subband_freq_hi_MHz=1.0e9, internal_nt=1024):
+    """Returns (freq_it0, freq_nt, freq_sd_off, sparse_data float32, it_start, it_end)."""
+    edges = np.asarray(freq_edges_MHz, np.float64)
+    var = np.asarray(freq_variances, np.float64)
+    nfreq, N = edges.size - 1, int(internal_nt)
+    dt = 1.0e-3 * time_sample_ms
+    nu0 = 0.5 * (edges[0] + edges[-1])
+    it0 = np.zeros(nfreq, np.int64)
+    nt = np.zeros(nfreq, np.int64)
+    off = np.zeros(nfreq, np.int64)
+    vals, snr_sq, total = [], 0.0, 0
+
+    def cum_at(cum, s):
+        if s < 1.0e-10:
+            return 0.0
+        if s > N - 1.0e-10:
+            return cum[N]
+        i = int(s)
+        return (1.0 - (s - i)) * cum[i] + (s - i) * cum[i + 1]
+
+    for f in range(nfreq):
+        lo, hi = edges[f], edges[f + 1]
+        off[f] = total
+        if hi <= subband_freq_lo_MHz or lo >= subband_freq_hi_MHz:
+            continue
+        nuc = 0.5 * (lo + hi)
+        d0 = 1.0e-3 * K_DM * dm / hi ** 2
+        d1 = 1.0e-3 * K_DM * dm / lo ** 2
+        dmw = d1 - d0
+        ts = 1.0e-3 * sm / (nuc / 1000.0) ** 4
+        t0 = d0 - 0.1 * dmw - 4.0 * intrinsic_width - ts
+        t1 = d1 + 0.1 * dmw + 4.0 * intrinsic_width + 10.0 * ts
+        tcen = 0.5 * (d0 + d1) - (t0 + (t1 - t0) / (2.0 * N))
+        om = (np.pi / (t1 - t0)) * np.arange(N + 1)
+        x = 0.5 * dmw * om
+        sinc = np.where(x * x > 1.0e-100, np.sin(x) / np.where(x == 0, 1.0, x), 1.0)
+        z = np.exp(-0.5 * (intrinsic_width * om) ** 2) * sinc / (1.0 + 1j * ts * om) * np.exp(-1j * tcen * om)
+        z[0] = z[0].real
+        z[N] = z[N].real
+        prof = np.fft.irfft(z, n=2 * N) * (2 * N)
+        cum = np.concatenate([[0.0], np.cumsum(np.maximum(prof[:N], 0.0))])
+        cum = cum / cum[N]
+        pt0, pt1 = undispersed_arrival_time_sec + t0, undispersed_arrival_time_sec + t1
+        i0, i1 = int(np.floor(pt0 / dt)), int(np.ceil(pt1 / dt))
+        it0[f], nt[f] = i0, i1 - i0
+        total += i1 - i0
+        amp = (nuc / nu0) ** spectral_index / dt
+        for it in range(i0, i1):
+            a = cum_at(cum, N * (it * dt - pt0) / (t1 - t0))
+            b = cum_at(cum, N * ((it + 1) * dt - pt0) / (t1 - t0))
+            v = amp * (b - a)
+            vals.append(np.float32(v))
+            snr_sq += v * v / var[f]
+    active = nt > 0
+    it_start = int(it0[active].min())
+    it_end = int((it0 + nt)[active].max())
+    it0[~active] = it_start
+    scale = snr / np.sqrt(snr_sq)
+    data = (np.array(vals, np.float64) * scale).astype(np.float32)
+    return it0, nt, off, data, it_start, it_end
