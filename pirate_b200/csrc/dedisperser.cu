@@ -252,7 +252,8 @@ void GpuDedisperser::allocate()
             vector<int> cap(nrows);
             long tot = 0;
             for (long row = 0; row < nrows; row++) {
-                cap[row] = int(round_up(plan.max_row_lag[p][row] + st.nt, 32));
+                // one sample more than the lags need: stage 2 also reads the sample before its first
+                cap[row] = int(round_up(plan.max_row_lag[p][row] + st.nt + 1, 32));
                 off[row] = tot;
                 tot += cap[row];
             }

@@ -534,11 +534,13 @@ __device__ __forceinline__ void bfly_l0_shared(float &v0, float &v1, float *h, i
 // All K steps of a register tree, in place. pv[r][q] holds pair q's row0 input of the previous tile.
 // With HS, the lag-0 pairs keep that history in shared memory (hs[slot], one float per pair, in
 // (r, q) order), which frees their registers. With EXT0, step 0 (all lags 0) takes its lag-1
-// operands from b0[q] = row 2q one sample earlier, supplied by the caller, and keeps no history.
-template<int K, bool HS = false, bool EXT0 = false>
+// operands from b0[q] = row 2q one sample earlier, supplied by the caller, and keeps no history;
+// with F0 the caller has already done step 0 itself (from rows it can read one sample earlier).
+template<int K, bool HS = false, bool EXT0 = false, bool F0 = false>
 __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>::NS][RT<K>::NP], int lane, float *hs = nullptr,
                                          const float *b0 = nullptr)
 {
+    static_assert(!F0 || EXT0, "a caller-done step 0 keeps no history (EXT0 layout)");
     int slot = 0;
 #pragma unroll
     for (int r = 0; r < K; r++) {
@@ -547,6 +549,8 @@ __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>
             const int h = 1 << r;
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
             const int L = rt_lag(r, q);
+            if (F0 && r == 0)
+                continue;
             if (EXT0 && r == 0) {
                 const float x = v[i0], y = v[i0 + 1];
                 v[i0] = bfly(x, y);
@@ -619,15 +623,17 @@ __device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP],
 // pf level r'+1 are emitted (FrequencySubbands multiplet order), reproducing ReferenceTree::dedisperse_2d
 // (src_lib/ReferenceTree.cpp:120-300): even band pairs coincide with the in-place butterflies, odd
 // ("staggered") pairs (2k+1, 2k+2) are extra butterflies with their own histories ps[r'][u].
-template<int RB, bool STAG, bool HS, bool EXT0, typename Emit>
+// With F0 the caller has done the level-0 emission and step 0's butterflies (not its emission).
+template<int RB, bool STAG, bool HS, bool EXT0, bool F0, typename Emit>
 __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv)[RT<RB>::NS][RT<RB>::NP],
                                                  float (&ps)[RT<RB>::NS][RT<RB>::NP], const Stage2Args &a,
                                                  int lane, Emit emit, float *hs, const float *b0)
 {
+    static_assert(!F0 || (EXT0 && !STAG), "a caller-done step 0: no history, no staggered pairs");
     constexpr int NB = 1 << RB;
     int slot = 0;   // HS: lag-0 in-place pairs keep their history in hs[slot] (see rt_steps)
     // Band counts are the same for every tile: each level's emission is skipped as a whole when empty.
-    if (a.sb_count[0] > 0) {
+    if (!F0 && a.sb_count[0] > 0) {
 #pragma unroll
         for (int f = 0; f < NB; f++)
             if (f < a.sb_count[0]) emit(a.sb_mbase[0] + f, v[f]);
@@ -658,7 +664,9 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
         for (int q = 0; q < RT<RB>::NP; q++) {
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
             const int L = rt_lag(r, q);
-            if (EXT0 && r == 0) {
+            if (F0 && r == 0) {
+                // done by the caller
+            } else if (EXT0 && r == 0) {
                 const float x = v[i0], y = v[i0 + 1];
                 v[i0] = bfly(x, y);
                 v[i0 + 1] = bfly(b0[q], y);
@@ -879,9 +887,14 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *hs = (float *) (sm_raw + Lay::hist) + warp * 16;   // this warp's lag-0 histories (HS)
-    // Phase-b step 0 reads its lag-1 operands from the shared delay line (stage 1; in stage 2 the
-    // extra live values cost more in register spills than the shuffles they save).
+    // Step 0 (all lags 0) without shuffles or histories. Stage 1, phase b: the lag-1 operands are read
+    // from the shared delay line. Stage 2: each phase does step 0 while it loads its rows, phase a
+    // reading each row from one sample earlier in the staging buffer (rows are staged from p - 1)
+    // and phase b from the delay line, so no extra values stay live.
     constexpr bool E0 = (STAGE == 1);
+    constexpr bool FA = (STAGE == 2) && (RA >= 1);
+    constexpr bool FB = (STAGE == 2) && !STAG && (RB >= 1);
+    constexpr bool EB = E0 || FB;
     const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
     float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
 
@@ -926,7 +939,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     if (is_a) {
         float pva[RT<RA>::NS][RT<RA>::NP];
         float *sta = st + RING + g * rt_state(RA);
-        rt_load<RA, HS>(pva, sta, lane, hs);
+        rt_load<RA, HS, FA>(pva, sta, lane, hs);
 
         // Issues the cp.async copies of this warp's NA rows for one tile into staging buffer 'buf',
         // then advances the rows' read positions by 32 samples.
@@ -945,12 +958,14 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 // Rows at their own positions: CPR consecutive 16-byte chunks from p & ~(EPC-1), consecutive
                 // lanes on consecutive chunks of a row. Capacities are multiples of 32 samples, so a chunk
                 // never straddles the end of a delay line and wraps at most once.
+                // With FA the run starts at p - 1 (32 + 1 samples fit in the same CPR chunks).
                 constexpr int EPC = Stage<Ts>::EPC, CPR = 32 / EPC + 1;
                 for (int c = lane; c < NA * CPR; c += 32) {
                     const int i = c / CPR, k = c - i * CPR, r = g * NA + i;
                     const int4 t = in_tab[r];
                     const int cap = t.y;
-                    int q = (t.x & ~(EPC - 1)) + k * EPC;
+                    const int p0 = FA ? ((t.x == 0) ? (cap - 1) : (t.x - 1)) : t.x;
+                    int q = (p0 & ~(EPC - 1)) + k * EPC;
                     q = (q >= cap) ? (q - cap) : q;
                     cp_async_bytes<16>(dst + i * SPRK + k * EPC, in + ((long) t.w << 32 | (unsigned) t.z) + q);
                 }
@@ -963,14 +978,14 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
             __syncwarp();
         };
 
-        // Stage 2: bits [OB i, OB i + OB) = offset of row i's first sample in its staged run,
-        // p & (EPC-1) (constant: positions advance by 32 and capacities are multiples of 32).
+        // Stage 2: bits [OB i, OB i + OB) = offset in its staged run of the first staged sample of row i,
+        // (p - FA) & (EPC-1) (constant: positions advance by 32 and capacities are multiples of 32).
         constexpr int OB = (sizeof(Ts) == 4) ? 2 : 3;
         unsigned long long offs = 0;
         if (STAGE == 2) {
 #pragma unroll
             for (int i = 0; i < NA; i++)
-                offs |= (unsigned long long) (in_tab[g * NA + i].x & (Stage<Ts>::EPC - 1)) << (OB * i);
+                offs |= (unsigned long long) ((in_tab[g * NA + i].x - (FA ? 1 : 0)) & (Stage<Ts>::EPC - 1)) << (OB * i);
         }
         issue(0);
         cp_async_commit();
@@ -983,10 +998,23 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 __syncwarp();
                 const Ts *sb = my_stage + (it & 1) * NB * NA * SPRK;
                 float v[NA];
+                if constexpr (FA) {
+                    // Step 0 while loading: pair (2q, 2q + 1), lag-1 operand = row 2q one sample earlier.
 #pragma unroll
-                for (int i = 0; i < NA; i++)
-                    v[i] = to_f(sb[i * SPRK + lane + int((offs >> (OB * i)) & ((1u << OB) - 1))]);
-                rt_steps<RA, HS>(v, pva, lane, hs);
+                    for (int q = 0; q < NA / 2; q++) {
+                        const Ts *r0 = sb + 2 * q * SPRK + lane + int((offs >> (OB * 2 * q)) & ((1u << OB) - 1));
+                        const Ts *r1 = sb + (2 * q + 1) * SPRK + lane + int((offs >> (OB * (2 * q + 1))) & ((1u << OB) - 1));
+                        const float xm = to_f(r0[0]), x = to_f(r0[1]), y = to_f(r1[1]);
+                        v[2 * q] = bfly(x, y);
+                        v[2 * q + 1] = bfly(xm, y);
+                    }
+                    rt_steps<RA, HS, true, true>(v, pva, lane, hs);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < NA; i++)
+                        v[i] = to_f(sb[i * SPRK + lane + int((offs >> (OB * i)) & ((1u << OB) - 1))]);
+                    rt_steps<RA, HS>(v, pva, lane, hs);
+                }
 #pragma unroll
                 for (int i = 0; i < NA; i++)
                     ring[tab_int<NA>(wb + g * NA, i) + lane] = v[i];
@@ -1002,11 +1030,11 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
             asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
         }
         cp_async_wait0();
-        rt_save<RA, HS>(pva, sta, lane, hs);
+        rt_save<RA, HS, FA>(pva, sta, lane, hs);
     } else {
         float pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
         float *stb = st + RING + NB * rt_state(RA) + g * (rt_state(RB) + (STAGE == 2 ? st_state(RB) : 0));
-        rt_load<RB, HS, E0>(pvb, stb, lane, hs);
+        rt_load<RB, HS, EB>(pvb, stb, lane, hs);
         if (STAG) st_load<RB>(psb, stb + rt_state(RB), lane);
 
         PfEmit<Ts> emit;
@@ -1025,16 +1053,40 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 // Phase-b rows, and (E0) for step 0 (lag 0) each even row one sample earlier: the delay
                 // line holds it (capacity >= P + 65), so no shuffle and no history are needed.
                 float v[NB], b0[RT<RB>::NP];
+                if constexpr (FB) {
+                    // Stage 2: level-0 emission and step 0 while loading (pair (f, f + 1), lag-1 operand
+                    // = row f one sample earlier, from the delay line).
+                    emit.row0 = pf_rows + pf_slot;
+                    pf_slot = (pf_slot + 32) & int(a.pf_cap - 1);
+                    const int cnt0 = a.sb_count[0], mb0 = a.sb_mbase[0];
 #pragma unroll
-                for (int f = 0; f < NB; f++) {
-                    const int2 t = tab_int2<NB>(rt + g * NB, f);
-                    const int lo = t.y & 0xffff, cap = t.y >> 16;
-                    int q = t.x + lane;
-                    q = (q < lo) ? (q + cap) : q;
-                    v[f] = ring[q];
-                    if (E0 && (f & 1) == 0 && RB > 0) {
-                        const int qm = (q == lo) ? (q + cap - 1) : (q - 1);
-                        b0[f >> 1] = ring[qm];
+                    for (int f = 0; f < NB; f += 2) {
+                        const int2 t0 = tab_int2<NB>(rt + g * NB, f), t1 = tab_int2<NB>(rt + g * NB, f + 1);
+                        const int lo0 = t0.y & 0xffff, cap0 = t0.y >> 16, lo1 = t1.y & 0xffff, cap1 = t1.y >> 16;
+                        int q0 = t0.x + lane, q1 = t1.x + lane;
+                        q0 = (q0 < lo0) ? (q0 + cap0) : q0;
+                        q1 = (q1 < lo1) ? (q1 + cap1) : q1;
+                        const int qm = (q0 == lo0) ? (q0 + cap0 - 1) : (q0 - 1);
+                        const float x = ring[q0], y = ring[q1], xm = ring[qm];
+                        if (cnt0 > 0) {
+                            if (f < cnt0) emit(mb0 + f, x);
+                            if (f + 1 < cnt0) emit(mb0 + f + 1, y);
+                        }
+                        v[f] = bfly(x, y);
+                        v[f + 1] = bfly(xm, y);
+                    }
+                } else {
+#pragma unroll
+                    for (int f = 0; f < NB; f++) {
+                        const int2 t = tab_int2<NB>(rt + g * NB, f);
+                        const int lo = t.y & 0xffff, cap = t.y >> 16;
+                        int q = t.x + lane;
+                        q = (q < lo) ? (q + cap) : q;
+                        v[f] = ring[q];
+                        if (E0 && (f & 1) == 0 && RB > 0) {
+                            const int qm = (q == lo) ? (q + cap - 1) : (q - 1);
+                            b0[f >> 1] = ring[qm];
+                        }
                     }
                 }
                 __syncwarp();
@@ -1057,15 +1109,17 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                         const int ob = out_base[i] + 32;
                         out_base[i] = (ob == out_off[i] + in_cap[i]) ? out_off[i] : ob;
                     }
+                } else if constexpr (FB) {
+                    phase_b_subbands<RB, STAG, HS, true, true>(v, pvb, psb, a, lane, emit, hs, b0);
                 } else {
                     emit.row0 = pf_rows + pf_slot;
                     pf_slot = (pf_slot + 32) & int(a.pf_cap - 1);
-                    phase_b_subbands<RB, STAG, HS, E0>(v, pvb, psb, a, lane, emit, hs, b0);
+                    phase_b_subbands<RB, STAG, HS, E0, false>(v, pvb, psb, a, lane, emit, hs, b0);
                 }
             }
             asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
         }
-        rt_save<RB, HS, E0>(pvb, stb, lane, hs);
+        rt_save<RB, HS, EB>(pvb, stb, lane, hs);
         if (STAG) st_save<RB>(psb, stb + rt_state(RB), lane);
     }
     __syncthreads();

@@ -124,7 +124,8 @@ void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, cons
         std::vector<int> cap(nrows);
         long tot = 0;
         for (long row = 0; row < nrows; row++) {
-            cap[row] = int(na_round_up(plan.max_row_lag[p][row] + st.nt, 32));
+            // one sample more than the lags need: stage 2 also reads the sample before its first
+            cap[row] = int(na_round_up(plan.max_row_lag[p][row] + st.nt + 1, 32));
             off[row] = tot;
             tot += cap[row];
         }
