@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import helpers as H
+import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -140,3 +141,45 @@ def test_fp32_bitwise_rank16(pb2lib):
         for i in range(orc.ntrees):
             assert np.array_equal(gres[seq][0][i], ores[seq][0][i]), "seq %d tree %d out_max" % (seq, i)
             assert np.array_equal(gres[seq][1][i], ores[seq][1][i]), "seq %d tree %d out_argmax" % (seq, i)
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float16"])
+def test_benchmark_config_full_size(pb2lib, dtype):
+    """The benchmark's workload at full size, one beam, two chunks, fed pirate's raw int4 input
+    through the fused dequantizing input path: rank-16 tree from 16384 channels, 5 primary trees
+    (time downsampling 1-16), widths to 32, full-band search. float32 storage: bitwise equal to the fp32
+    oracle on the dequantized input. float16 storage (the benchmark's): within the fp16 tolerance
+    of 1e-2 sigma (bare weights), and every GPU token re-evaluates in the oracle to within 2e-2."""
+    import torch
+    import bench
+    cfg = bench.bench_config(1, dtype)
+    rng = np.random.default_rng(77)
+    B, F, T = 1, 16384, cfg["time_samples_per_chunk"]
+    qs = [O.random_quantized(rng, B, F, T) for _ in range(2)]
+    xs = [O.dequantize(d, s, B, F, T) for d, s in qs]
+    orc = O.OracleDedisperser(cfg, 1, 32)         # one instance: about 20 GB of lag state at rank 16
+    ws = [O.bare_weights(orc.wt_shape(i), orc.trees[i]["nprofiles"])[None] for i in range(orc.ntrees)]
+    ores = [orc.dedisperse(0, x, [w[0] for w in ws]) for x in xs]
+    plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(cfg))
+    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=1)
+    dd.allocate()
+    for i, w in enumerate(ws):
+        dd.fill_all_weights(i, w)
+    for seq, (d, s) in enumerate(qs):
+        with dd.get_input_int4() as (dq, sq):
+            dq.copy_(torch.from_numpy(d).cuda())
+            sq.copy_(torch.from_numpy(s).cuda())
+        with dd.get_output(0, sync=True) as out:
+            for i in range(orc.ntrees):
+                gm = out.out_max[i].float().cpu().numpy().astype(np.float64)
+                ga = out.out_argmax[i].cpu().numpy().view(np.uint32)
+                om, oa = ores[seq][0][i], ores[seq][1][i]
+                if dtype == "float32":
+                    assert np.array_equal(gm, om), "seq %d tree %d out_max" % (seq, i)
+                    assert np.array_equal(ga, oa), "seq %d tree %d out_argmax" % (seq, i)
+                else:
+                    err = float(np.abs(gm - om).max())
+                    assert err <= 1e-2, "seq %d tree %d: max |gpu - oracle| = %.3g sigma" % (seq, i, err)
+                    if seq == len(qs) - 1:
+                        ev = orc.eval_tokens(i, ga, ws[i][0])
+                        assert np.abs(ev - om).max() <= 2e-2, "tree %d: tokens" % i
