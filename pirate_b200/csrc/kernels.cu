@@ -1453,6 +1453,12 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
     int winG = -1;            // group l * M + m of the first maximum; -1: no trial above -1e30
     float outv = best;        // value and token of the first maximal trial
     uint32_t tok = 0xffffffffu;
+    // Inputs of the winning group's first maximal pair, saved when the maximum moves, so that the
+    // token is found once at the end: x[j - 3S .. j] of its samples is = winP (a) and winP + 1 (b),
+    // the level's weights, and the pair's level, multiplet and start.
+    float xa0 = 0, xa1 = 0, xa2 = 0, xa3 = 0, xb0 = 0, xb1 = 0, xb2 = 0, xb3 = 0;
+    float sw0 = 0, sw1 = 0, sw2 = 0, sw3 = 0;
+    int winL = 0, winM = 0, winP = 0;
 
     // The window's raw samples are staged with cp.async one multiplet ahead (4-sample runs: a
     // 4-aligned run never wraps the delay line).
@@ -1489,8 +1495,6 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
             __syncwarp();
             wsm_n = n;
         }
-        bool upd = false;     // this lane's maximum moved to a group of this multiplet
-        int winL = 0, winP = 0;
 #pragma unroll
         for (int l = 0; l < L; l++) {
             const int S = g.S[l], nsamp = g.nsamp[l];
@@ -1606,48 +1610,55 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
             if (gmax > best || (gmax == best && G < winG)) {
                 best = gmax;
                 winG = G;
-                upd = true;
                 winL = l;
+                winM = m;
                 winP = gp;
+                const int S = g.S[l];
+                const int j = g.I[l] + lane * nsamp + gp;
+                xa3 = lev[pf_phys(g, l, j)];
+                if (full) {
+                    xa2 = lev[pf_phys(g, l, j - S)];
+                    xa1 = lev[pf_phys(g, l, j - 2 * S)];
+                    xa0 = lev[pf_phys(g, l, j - 3 * S)];
+                }
+                if (gp + 1 < nsamp) {
+                    xb3 = lev[pf_phys(g, l, j + 1)];
+                    if (full) {
+                        xb2 = lev[pf_phys(g, l, j + 1 - S)];
+                        xb1 = lev[pf_phys(g, l, j + 1 - 2 * S)];
+                        xb0 = lev[pf_phys(g, l, j + 1 - 3 * S)];
+                    }
+                }
+                sw0 = w0; sw1 = w1; sw2 = w2; sw3 = w3;
             }
         }
 
-        // A lane whose maximum moved to this multiplet recomputes the trials of the winning group's
-        // first maximal fine sample (or pair) from the levels still in shared memory, in the
-        // reference's order (fine time, then profile 0, 3l+1, 3l+2, 3l+3); the first equal to the
-        // maximum gives the output value and token.
-        if (__any_sync(0xffffffffu, upd)) {
-            if (upd) {
-                const int l = winL;
-                const int dt = gr.dt[l], S = gr.S[l], nsamp = gr.nsamp[l];
-                const int j0 = gr.I[l] + lane * nsamp;
-                const float w0 = (l == 0) ? wsm[tl] : 0.0f;
-                const float w1 = full ? wsm[(3 * l + 1) * 32 + tl] : 0.0f;
-                const float w2 = full ? wsm[(3 * l + 2) * 32 + tl] : 0.0f;
-                const float w3 = full ? wsm[(3 * l + 3) * 32 + tl] : 0.0f;
-                for (int is = winP; is < min(winP + 2, nsamp); is++) {
-                    const int j = j0 + is;
-                    const float x3 = lev[pf_phys(gr, l, j)];
-                    const uint32_t tk0 = (uint32_t(m) << 16) | uint32_t(is * dt);
-                    if (l == 0) {
-                        const float v0 = __fmul_rn(w0, x3);
-                        if (v0 == best) { outv = v0; tok = tk0; break; }
-                    }
-                    if (full) {
-                        const float x0 = lev[pf_phys(gr, l, j - 3 * S)];
-                        const float x1 = lev[pf_phys(gr, l, j - 2 * S)];
-                        const float x2 = lev[pf_phys(gr, l, j - S)];
-                        const float hx3 = __fmul_rn(0.5f, x3);
-                        const float v1 = __fmul_rn(w1, __fadd_rn(x2, x3));
-                        const float v2 = __fmul_rn(w2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3));
-                        const float v3 = __fmul_rn(w3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3));
-                        if (v1 == best) { outv = v1; tok = tk0 | (uint32_t(3 * l + 1) << 8); break; }
-                        if (v2 == best) { outv = v2; tok = tk0 | (uint32_t(3 * l + 2) << 8); break; }
-                        if (v3 == best) { outv = v3; tok = tk0 | (uint32_t(3 * l + 3) << 8); break; }
-                    }
-                }
+    }
+
+    // The first trial of the winning pair, in the reference's order (fine time, then profile 0, 3l+1,
+    // 3l+2, 3l+3), equal to the maximum gives the output value and token.
+    if (winG >= 0) {
+        const int l = winL;
+        const uint32_t dt = uint32_t(gr.dt[l]);
+        const int nsamp = gr.nsamp[l];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            if (k == 1 && winP + 1 >= nsamp) break;
+            const float x3 = k ? xb3 : xa3, x2 = k ? xb2 : xa2, x1 = k ? xb1 : xa1, x0 = k ? xb0 : xa0;
+            const uint32_t tk0 = (uint32_t(winM) << 16) | (uint32_t(winP + k) * dt);
+            if (l == 0) {
+                const float v0 = __fmul_rn(sw0, x3);
+                if (v0 == best) { outv = v0; tok = tk0; break; }
             }
-            __syncwarp();
+            if (full) {
+                const float hx3 = __fmul_rn(0.5f, x3);
+                const float v1 = __fmul_rn(sw1, __fadd_rn(x2, x3));
+                const float v2 = __fmul_rn(sw2, __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x1), x2), hx3));
+                const float v3 = __fmul_rn(sw3, __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), x1), x2), hx3));
+                if (v1 == best) { outv = v1; tok = tk0 | (uint32_t(3 * l + 1) << 8); break; }
+                if (v2 == best) { outv = v2; tok = tk0 | (uint32_t(3 * l + 2) << 8); break; }
+                if (v3 == best) { outv = v3; tok = tk0 | (uint32_t(3 * l + 3) << 8); break; }
+            }
         }
     }
 
