@@ -1328,7 +1328,8 @@ struct PfGeom
     int rr[kPfMaxLevels], ss[kPfMaxLevels];   // B_l[u] = B_{l-1}[rr u] + B_{l-1}[rr u + ss]
     int flags[kPfMaxLevels]; // kPfU: dt = 2^l; kPfPairs: scanned two fine samples at a time;
                              // kPfNextU: level l+1 has dt = 2^(l+1) and is built by this level's scan
-    int raw_off;             // staging buffer of the window's raw samples (16-byte aligned)
+    int raw_off;             // two staging buffers of the window's raw samples (16-byte aligned), one per
+    int raw_floats;          // multiplet in flight, raw_floats apart; level 0 is read from them directly
     int w_off;               // the warp's weights of one subband, [profile < 16][weight time < 32]
     int warp_floats;
 };
@@ -1365,6 +1366,27 @@ template<> __device__ __forceinline__ void pf_load4<__nv_bfloat16>(const __nv_bf
     const float2 a = __bfloat1622float2(*(const __nv_bfloat162 *) &q.x), b = __bfloat1622float2(*(const __nv_bfloat162 *) &q.y);
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
+// Eight samples from a 16-byte-aligned address (two 4-sample loads for fp32).
+template<typename Ts> __device__ __forceinline__ void pf_load8(const Ts *p, float (&v)[8])
+{
+    if constexpr (sizeof(Ts) == 4) {
+        float a[4], b[4];
+        pf_load4<Ts>(p, a);
+        pf_load4<Ts>(p + 4, b);
+#pragma unroll
+        for (int i = 0; i < 4; i++) { v[i] = a[i]; v[4 + i] = b[i]; }
+    } else {
+        const uint4 q = *(const uint4 *) p;
+        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            float2 f;
+            if constexpr (std::is_same<Ts, __half>::value) f = __half22float2(*(const __half2 *) &w[i]);
+            else f = __bfloat1622float2(*(const __nv_bfloat162 *) &w[i]);
+            v[2 * i] = f.x; v[2 * i + 1] = f.y;
+        }
+    }
+}
 
 // Shared-memory layout of the fast peak finder for one warp (see PfGeom).
 __host__ __device__ constexpr PfGeom pf_geom(int Dout, int Dcore, int tpad, int L, int esize)
@@ -1398,11 +1420,12 @@ __host__ __device__ constexpr PfGeom pf_geom(int Dout, int Dcore, int tpad, int 
                    | ((l + 1 < L && (2 << l) <= Dcore) ? kPfNextU : 0);
         const int t = g.n[l] - 1 + g.e[l];
         const int size = t + g.pad[l] * (t >> k) + 1;
-        off += (size + 1) & ~1;
+        if (l > 0)   // level 0 lives only in the raw staging buffer
+            off += (size + 1) & ~1;
     }
     g.raw_off = (off + 3) & ~3;
-    const int raw_floats = ((32 * Dout + tpad) * esize + 15) / 16 * 4;
-    g.w_off = g.raw_off + raw_floats;
+    g.raw_floats = ((32 * Dout + tpad) * esize + 15) / 16 * 4;
+    g.w_off = g.raw_off + 2 * g.raw_floats;
     g.warp_floats = g.w_off + kPfMaxProfiles * 32;
     return g;
 }
@@ -1460,11 +1483,13 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
     float sw0 = 0, sw1 = 0, sw2 = 0, sw3 = 0;
     int winL = 0, winM = 0, winP = 0;
 
-    // The window's raw samples are staged with cp.async one multiplet ahead (4-sample runs: a
-    // 4-aligned run never wraps the delay line).
-    Ts *raw = (Ts *) (lev + g.raw_off);
+    // The window's raw samples are staged with cp.async one multiplet ahead into alternating buffers
+    // (4-sample runs: a 4-aligned run never wraps the delay line). Level 0 is read from them.
+    Ts *raw0 = (Ts *) (lev + g.raw_off);
+    const int raw_ts = g.raw_floats * int(sizeof(float) / sizeof(Ts));
     auto stage = [&](int m) {
         const Ts *row = pfrows + (long) m * a.pf_cap;
+        Ts *raw = raw0 + (m & 1) * raw_ts;
         for (int q = lane; q < nq0; q += 32)
             cp_async_bytes<4 * sizeof(Ts)>(raw + 4 * q, row + ((sbm + 4 * q) & mask));
         cp_async_commit();
@@ -1472,19 +1497,13 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
     stage(0);
 
     for (int m = 0; m < a.M; m++) {
-        // Level 0: the window's samples from the staging buffer; then stage the next multiplet.
+        // Wait for this multiplet's samples; then stage the next one into the other buffer (every
+        // lane is past its reads of that buffer: they came before this loop's previous barriers).
         cp_async_wait0();
-        __syncwarp();
-        for (int q = lane; q < nq0; q += 32) {
-            float v[4];
-            pf_load4<Ts>(raw + 4 * q, v);
-            float *d = lev + pf_phys(g, 0, 4 * q);
-            *(float2 *) d = make_float2(v[0], v[1]);
-            *(float2 *) (d + 2) = make_float2(v[2], v[3]);
-        }
         __syncwarp();
         if (m + 1 < a.M)
             stage(m + 1);
+        const Ts *rawc = raw0 + (m & 1) * raw_ts;
 
         const int n = a.m_to_n[m];
         if (n != wsm_n) {
@@ -1511,7 +1530,8 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
             if (nextU) {
                 // Entries of level l+1 before the first output time.
                 for (int u = lane; u < g.I[l + 1]; u += 32)
-                    lev[pf_phys(g, l + 1, u)] = __fadd_rn(lev[pf_phys(g, l, 2 * u)], lev[pf_phys(g, l, 2 * u + 1)]);
+                    lev[pf_phys(g, l + 1, u)] = (l == 0) ? __fadd_rn(to_f(rawc[2 * u]), to_f(rawc[2 * u + 1]))
+                                                        : __fadd_rn(lev[pf_phys(g, l, 2 * u)], lev[pf_phys(g, l, 2 * u + 1)]);
             }
 
             float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f;
@@ -1527,20 +1547,27 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
             int gp = 0;   // first fine sample (pair start) whose trials reach gmax
             if (g.flags[l] & kPfPairs) {
                 // x0..x3 = x[is-3..is]; carried: x2, hx1 = x[is-2]/2, hx2 = x[is-1]/2, Ap = x[is-3]/2 + x[is-2].
-                float x2 = lev[pf_phys(g, l, j0 - 1)];
-                const float x1 = lev[pf_phys(g, l, j0 - 2)];
-                const float x0 = lev[pf_phys(g, l, j0 - 3)];
+                // Level 0 comes from the raw staging buffer (entry i = raw sample i; j0 is a multiple of 4).
+                float x2, x1, x0;
+                if (l == 0) {
+                    float q[4];
+                    pf_load4<Ts>(rawc + j0 - 4, q);
+                    x0 = q[1]; x1 = q[2]; x2 = q[3];
+                } else {
+                    x2 = lev[pf_phys(g, l, j0 - 1)];
+                    x1 = lev[pf_phys(g, l, j0 - 2)];
+                    x0 = lev[pf_phys(g, l, j0 - 3)];
+                }
                 float2 H = make_float2(__fmul_rn(0.5f, x1), __fmul_rn(0.5f, x2));   // x[is-2]/2, x[is-1]/2
                 float Ap = __fadd_rn(__fmul_rn(0.5f, x0), x1);
-                const float *xs = lev + pf_phys(g, l, j0);
+                const float *xs = lev + ((l > 0) ? pf_phys(g, l, j0) : 0);
                 float *ys = lev + (nextU ? pf_phys(g, l + 1, g.I[l + 1] + lane * (nsamp >> 1)) : 0);
                 const float2 W0 = make_float2(w0, w0), W1 = make_float2(w1, w1);
                 const float2 W2 = make_float2(w2, w2), W3 = make_float2(w3, w3);
 
-#pragma unroll 2
-                for (int is = 0; is < nsamp; is += 2) {
-                    const float2 X = *(const float2 *) (xs + is);
-                    const float xa = X.x, xb = X.y;
+                // The trials of fine samples is (xa) and is + 1 (xb).
+                auto pair = [&](const float xa, const float xb, const int is) {
+                    const float2 X = make_float2(xa, xb);
                     float mx;
                     if (full) {
                         // Fine samples is (xa) and is+1 (xb), in packed pairs (a, b): profiles
@@ -1565,6 +1592,32 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
                     }
                     if (mx > gmax) { gmax = mx; gp = is; }
                     if (nextU) ys[is >> 1] = __fadd_rn(xa, xb);
+                };
+                if (l == 0) {
+                    // 16-byte loads when runs of 8 stay 16-byte aligned (tpad and Dout multiples of 8)
+                    if (DOUT > 0 && nsamp % 8 == 0 && pf_tpad_of(L) % 8 == 0) {
+                        for (int is = 0; is < nsamp; is += 8) {
+                            float q[8];
+                            pf_load8<Ts>(rawc + j0 + is, q);
+                            pair(q[0], q[1], is);
+                            pair(q[2], q[3], is + 2);
+                            pair(q[4], q[5], is + 4);
+                            pair(q[6], q[7], is + 6);
+                        }
+                    } else {
+                        for (int is = 0; is < nsamp; is += 4) {
+                            float q[4];
+                            pf_load4<Ts>(rawc + j0 + is, q);
+                            pair(q[0], q[1], is);
+                            pair(q[2], q[3], is + 2);
+                        }
+                    }
+                } else {
+#pragma unroll 2
+                    for (int is = 0; is < nsamp; is += 2) {
+                        const float2 X = *(const float2 *) (xs + is);
+                        pair(X.x, X.y, is);
+                    }
                 }
             } else {
                 // Levels stored without padding (contiguous across lanes): x[j - k S] = xb[is - k S].
@@ -1615,18 +1668,20 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
                 winP = gp;
                 const int S = g.S[l];
                 const int j = g.I[l] + lane * nsamp + gp;
-                xa3 = lev[pf_phys(g, l, j)];
+                // level l's entry i (level 0: the raw sample)
+                auto X = [&](int i) { return (l == 0) ? to_f(rawc[i]) : lev[pf_phys(g, l, i)]; };
+                xa3 = X(j);
                 if (full) {
-                    xa2 = lev[pf_phys(g, l, j - S)];
-                    xa1 = lev[pf_phys(g, l, j - 2 * S)];
-                    xa0 = lev[pf_phys(g, l, j - 3 * S)];
+                    xa2 = X(j - S);
+                    xa1 = X(j - 2 * S);
+                    xa0 = X(j - 3 * S);
                 }
                 if (gp + 1 < nsamp) {
-                    xb3 = lev[pf_phys(g, l, j + 1)];
+                    xb3 = X(j + 1);
                     if (full) {
-                        xb2 = lev[pf_phys(g, l, j + 1 - S)];
-                        xb1 = lev[pf_phys(g, l, j + 1 - 2 * S)];
-                        xb0 = lev[pf_phys(g, l, j + 1 - 3 * S)];
+                        xb2 = X(j + 1 - S);
+                        xb1 = X(j + 1 - 2 * S);
+                        xb0 = X(j + 1 - 3 * S);
                     }
                 }
                 sw0 = w0; sw1 = w1; sw2 = w2; sw3 = w3;
