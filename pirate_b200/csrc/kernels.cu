@@ -933,6 +933,20 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     const int g = is_a ? warp : (warp - NB);   // phase-a group (f) or phase-b group (d)
     const int ntiles = a.nt / 32;
     __syncthreads();
+    // Register splits between the warp roles (whole warpgroups: phase a is warps 0-15). Each block is
+    // launched with the kernel's allocation, and the split adds up to exactly that, so the increase
+    // is always satisfied once phase a has decreased, which every phase-a warp does here before any
+    // barrier:
+    //   4+4 (1024 threads, 64 registers): 56 x 512 (phase a) + 72 x 512 (phase b) = 64 x 1024;
+    //   3+4 (768 threads, 80 registers): 72 x 512 (phase a) + 96 x 256 (phase b) = 80 x 768.
+    if constexpr (RA == 4 && RB == 4) {
+        if (is_a) asm volatile("setmaxnreg.dec.sync.aligned.u32 56;");
+        else asm volatile("setmaxnreg.inc.sync.aligned.u32 72;");
+    }
+    if constexpr (RA == 3 && RB == 4) {
+        if (is_a) asm volatile("setmaxnreg.dec.sync.aligned.u32 72;");
+        else asm volatile("setmaxnreg.inc.sync.aligned.u32 96;");
+    }
 
     // The two warp roles run separate loops (so each holds only its own histories in registers);
     // they meet once per tile at named barrier 1.
