@@ -934,12 +934,17 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     const int ntiles = a.nt / 32;
     __syncthreads();
     // Register splits between the warp roles (whole warpgroups: phase a is warps 0-15). Each block is
-    // launched with the kernel's allocation, and the split adds up to exactly that, so the increase
-    // is always satisfied once phase a has decreased, which every phase-a warp does here before any
-    // barrier:
-    //   4+4 (1024 threads, 64 registers): 56 x 512 (phase a) + 72 x 512 (phase b) = 64 x 1024;
+    // launched with the kernel's allocation, and the split adds up to exactly that, so the increasing
+    // role's request is always satisfied once the other role has decreased, which each of its warps
+    // does here before any barrier:
+    //   4+4 (1024 threads, 64 registers): stage 1: 72 x 512 (phase a) + 56 x 512 (phase b) = 64 x 1024,
+    //        stage 2: 56 x 512 (phase a) + 72 x 512 (phase b);
     //   3+4 (768 threads, 80 registers): 72 x 512 (phase a) + 96 x 256 (phase b) = 80 x 768.
-    if constexpr (RA == 4 && RB == 4) {
+    if constexpr (RA == 4 && RB == 4 && STAGE == 1) {
+        if (is_a) asm volatile("setmaxnreg.inc.sync.aligned.u32 72;");
+        else asm volatile("setmaxnreg.dec.sync.aligned.u32 56;");
+    }
+    if constexpr (RA == 4 && RB == 4 && STAGE == 2) {
         if (is_a) asm volatile("setmaxnreg.dec.sync.aligned.u32 56;");
         else asm volatile("setmaxnreg.inc.sync.aligned.u32 72;");
     }
@@ -953,7 +958,10 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     if (is_a) {
         float pva[RT<RA>::NS][RT<RA>::NP];
         float *sta = st + RING + g * rt_state(RA);
-        rt_load<RA, HS, FA>(pva, sta, lane, hs);
+        // Stage 1's phase a keeps its lag-0 histories in registers (room after the split; measured
+        // faster); stage 2's, with 56 registers, in shared memory.
+        constexpr bool HSA = HS && !(STAGE == 1 && RB == 4 && (RA == 4 || RA == 3));
+        rt_load<RA, HSA, FA>(pva, sta, lane, hs);
 
         // Issues the cp.async copies of this warp's NA rows for one tile into staging buffer 'buf',
         // then advances the rows' read positions by 32 samples.
@@ -1022,12 +1030,12 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                         v[2 * q] = bfly(x, y);
                         v[2 * q + 1] = bfly(xm, y);
                     }
-                    rt_steps<RA, HS, true, true>(v, pva, lane, hs);
+                    rt_steps<RA, HSA, true, true>(v, pva, lane, hs);
                 } else {
 #pragma unroll
                     for (int i = 0; i < NA; i++)
                         v[i] = to_f(sb[i * SPRK + lane + int((offs >> (OB * i)) & ((1u << OB) - 1))]);
-                    rt_steps<RA, HS>(v, pva, lane, hs);
+                    rt_steps<RA, HSA>(v, pva, lane, hs);
                 }
 #pragma unroll
                 for (int i = 0; i < NA; i++)
@@ -1044,7 +1052,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
             asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
         }
         cp_async_wait0();
-        rt_save<RA, HS, FA>(pva, sta, lane, hs);
+        rt_save<RA, HSA, FA>(pva, sta, lane, hs);
     } else {
         float pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
         float *stb = st + RING + NB * rt_state(RA) + g * (rt_state(RB) + (STAGE == 2 ? st_state(RB) : 0));
