@@ -138,8 +138,10 @@ __device__ __forceinline__ void store_run(Ts *p, const float (&o)[W])
 // add with (scale, offset) converted from fp16. The result is then rounded once to the output type.
 __device__ __forceinline__ float dq_value(uint32_t nib, float scale, float offset)
 {
-    const int v = int(nib & 0xf) - int((nib & 8) << 1);
-    return (v == -8) ? 0.0f : __fadd_rn(__fmul_rn(scale, float(v)), offset);
+    // u = v + 8 in [0, 15]; 2^23 + u is exact in fp32, so subtracting 2^23 + 8 gives v exactly.
+    const uint32_t u = (nib & 0xf) ^ 8u;
+    const float fv = __fsub_rn(__uint_as_float(0x4B000000u + u), 8388616.0f);
+    return (u == 0) ? 0.0f : __fadd_rn(__fmul_rn(scale, fv), offset);
 }
 
 // W consecutive samples from t0 of one int4 row (row = the row's bytes, so = its (scale, offset)
