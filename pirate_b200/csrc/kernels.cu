@@ -939,14 +939,14 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     // launched with the kernel's allocation, and the split adds up to exactly that, so the increasing
     // role's request is always satisfied once the other role has decreased, which each of its warps
     // does here before any barrier:
-    //   4+4 (1024 threads, 64 registers): stage 1: 72 x 512 (phase a) + 56 x 512 (phase b) = 64 x 1024,
-    //        stage 2: 56 x 512 (phase a) + 72 x 512 (phase b);
+    //   4+4 (1024 threads, 64 registers): 72 x 512 (phase a) + 56 x 512 (phase b) = 64 x 1024, or
+    //        56 x 512 + 72 x 512 for stage 2 with staggered subband pairs (phase b's extra histories);
     //   3+4 (768 threads, 80 registers): 72 x 512 (phase a) + 96 x 256 (phase b) = 80 x 768.
-    if constexpr (RA == 4 && RB == 4 && STAGE == 1) {
+    if constexpr (RA == 4 && RB == 4 && !(STAGE == 2 && STAG)) {
         if (is_a) asm volatile("setmaxnreg.inc.sync.aligned.u32 72;");
         else asm volatile("setmaxnreg.dec.sync.aligned.u32 56;");
     }
-    if constexpr (RA == 4 && RB == 4 && STAGE == 2) {
+    if constexpr (RA == 4 && RB == 4 && STAGE == 2 && STAG) {
         if (is_a) asm volatile("setmaxnreg.dec.sync.aligned.u32 56;");
         else asm volatile("setmaxnreg.inc.sync.aligned.u32 72;");
     }
@@ -960,9 +960,9 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     if (is_a) {
         float pva[RT<RA>::NS][RT<RA>::NP];
         float *sta = st + RING + g * rt_state(RA);
-        // Stage 1's phase a keeps its lag-0 histories in registers (room after the split; measured
-        // faster); stage 2's, with 56 registers, in shared memory.
-        constexpr bool HSA = HS && !(STAGE == 1 && RB == 4 && (RA == 4 || RA == 3));
+        // Phase a keeps its lag-0 histories in registers where the split gives it the room (measured
+        // faster); with staggered subbands it has 56 registers and keeps them in shared memory.
+        constexpr bool HSA = HS && !(RB == 4 && (RA == 4 || RA == 3) && !(STAGE == 2 && STAG));
         rt_load<RA, HSA, FA>(pva, sta, lane, hs);
 
         // Issues the cp.async copies of this warp's NA rows for one tile into staging buffer 'buf',
@@ -1058,10 +1058,9 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     } else {
         float pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
         float *stb = st + RING + NB * rt_state(RA) + g * (rt_state(RB) + (STAGE == 2 ? st_state(RB) : 0));
-        // Stage 2's phase b keeps its lag-0 histories in registers (it has the room after the split;
-        // measured 1.5% faster) unless it also runs staggered pairs; stage 1's stay in shared memory
-        // (measured faster there).
-        constexpr bool HSB = HS && (STAGE == 1 || STAG);
+        // Phase b keeps its lag-0 histories in shared memory (56 registers, or 72 with staggered pairs,
+        // whose own histories take the room).
+        constexpr bool HSB = HS;
         rt_load<RB, HSB, EB>(pvb, stb, lane, hs);
         if (STAG) st_load<RB>(psb, stb + rt_state(RB), lane);
 
