@@ -1059,8 +1059,8 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
         float pvb[RT<RB>::NS][RT<RB>::NP], psb[RT<RB>::NS][RT<RB>::NP];
         float *stb = st + RING + NB * rt_state(RA) + g * (rt_state(RB) + (STAGE == 2 ? st_state(RB) : 0));
         // Phase b keeps its lag-0 histories in shared memory (56 registers, or 72 with staggered pairs,
-        // whose own histories take the room).
-        constexpr bool HSB = HS;
+        // whose own histories take the room), except in the 3+4 trees, where it has 96.
+        constexpr bool HSB = HS && !(RA == 3 && RB == 4);
         rt_load<RB, HSB, EB>(pvb, stb, lane, hs);
         if (STAG) st_load<RB>(psb, stb + rt_state(RB), lane);
 
