@@ -1080,12 +1080,16 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 // Phase-b rows, and (E0) for step 0 (lag 0) each even row one sample earlier: the delay
                 // line holds it (capacity >= P + 65), so no shuffle and no history are needed.
                 float v[NB], b0[RT<RB>::NP];
-                if constexpr (FB) {
-                    // Stage 2: level-0 emission and step 0 while loading (pair (f, f + 1), lag-1 operand
-                    // = row f one sample earlier, from the delay line).
-                    emit.row0 = pf_rows + pf_slot;
-                    pf_slot = (pf_slot + 32) & int(a.pf_cap - 1);
-                    const int cnt0 = a.sb_count[0], mb0 = a.sb_mbase[0];
+                if constexpr (FB || (STAGE == 1 && RB >= 1)) {
+                    // Step 0 while loading (pair (f, f + 1), lag-1 operand = row f one sample earlier,
+                    // from the delay line), and in stage 2 the level-0 emission.
+                    int cnt0 = 0, mb0 = 0;
+                    if constexpr (STAGE == 2) {
+                        emit.row0 = pf_rows + pf_slot;
+                        pf_slot = (pf_slot + 32) & int(a.pf_cap - 1);
+                        cnt0 = a.sb_count[0];
+                        mb0 = a.sb_mbase[0];
+                    }
 #pragma unroll
                     for (int f = 0; f < NB; f += 2) {
                         const int2 t0 = tab_int2<NB>(rt + g * NB, f), t1 = tab_int2<NB>(rt + g * NB, f + 1);
@@ -1095,7 +1099,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                         q1 = (q1 < lo1) ? (q1 + cap1) : q1;
                         const int qm = (q0 == lo0) ? (q0 + cap0 - 1) : (q0 - 1);
                         const float x = ring[q0], y = ring[q1], xm = ring[qm];
-                        if (cnt0 > 0) {
+                        if (STAGE == 2 && cnt0 > 0) {
                             if (f < cnt0) emit(mb0 + f, x);
                             if (f + 1 < cnt0) emit(mb0 + f + 1, y);
                         }
@@ -1125,7 +1129,10 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                     rt[rr].x = (x >= lo + cap - ring_lag<RA, RB>(lane, g)) ? (x - cap) : x;
                 }
                 if constexpr (STAGE == 1) {
-                    rt_steps<RB, HSB, E0>(v, pvb, lane, hs, b0);
+                    if constexpr (RB >= 1)
+                        rt_steps<RB, HSB, true, true>(v, pvb, lane, hs);
+                    else
+                        rt_steps<RB, HSB, E0>(v, pvb, lane, hs, b0);
                     Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride + a.ring_off[(long) blk * NR];
 #pragma unroll
                     for (int f = 0; f < NB; f++)
