@@ -121,3 +121,55 @@ def test_plan_rejects_bad_downsampling(pb2lib):
     with pytest.raises(Exception) as e:
         pb2lib.DedispersionPlan(cfg)
     assert "dm_downsampling" in str(e.value)
+
+
+def test_new_entry_points_validate_arguments(pb2lib):
+    """Argument checks of the analytic-weight, grouper and pulse entry points run before any device
+    work, so they report errors (status != 0 and a message) without a GPU."""
+    import numpy as np
+    L = pb2lib.lib()
+    from pirate_b200 import simpulse
+    simpulse._sigs()
+    plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(H.toy_config(rank=6, nfreq=100, nt=256)))
+    vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+
+    def fails(rc, word):
+        msg = L.pb2_last_error().decode()
+        assert rc != 0 and word in msg, msg
+
+    # PfAvarApproximation: wrong tree count, wrong output length, null pointers
+    fv = np.ones(plan.nfreq)
+    outs = [np.zeros(t.nsubbands * t.ndm_wt * t.nprofiles) for t in plan.trees]
+    ptrs = (dp * plan.ntrees)(*[o.ctypes.data_as(dp) for o in outs])
+    lens = (ctypes.c_long * plan.ntrees)(*[o.size for o in outs])
+    assert L.pb2_plan_pf_variances(plan._h, fv.ctypes.data_as(dp), fv.size, ptrs, lens, plan.ntrees) == 0
+    fails(L.pb2_plan_pf_variances(plan._h, fv.ctypes.data_as(dp), fv.size, ptrs, lens, plan.ntrees + 1), "ntrees")
+    lens[0] += 1
+    fails(L.pb2_plan_pf_variances(plan._h, fv.ctypes.data_as(dp), fv.size, ptrs, lens, plan.ntrees), "out[0]")
+    fails(L.pb2_plan_pf_variances(plan._h, None, fv.size, ptrs, lens, plan.ntrees), "null")
+    fails(L.pb2_dd_fill_analytic_weights(None, fv.ctypes.data_as(dp), fv.size), "null")
+    fails(L.pb2_plan_tree_subbands(plan._h, 0, (ctypes.c_long * 9)(), (ctypes.c_long * 9)(), 9), "subbands")
+    # batch decoders: empty input
+    z = np.zeros(1, np.int64)
+    fails(L.pb2_plan_decode_argmax_batch(plan._h, 0, z.ctypes.data, *[z.ctypes.data] * 3, *[z.ctypes.data] * 5), "nonempty")
+    # beam peaks: null outputs, bad tree count, bad dtype
+    o = pb2lib._Outputs()
+    buf = np.zeros(64, np.float32)
+    fails(L.pb2_beam_peaks(None, *[buf.ctypes.data] * 5, None), "null")
+    o.ntrees = 0
+    fails(L.pb2_beam_peaks(ctypes.byref(o), *[buf.ctypes.data] * 5, None), "ntrees")
+    o.ntrees, o.nbeams, o.dtype = 1, 1, 7
+    o.ndm_out[0], o.nt_out[0] = 2, 2
+    o.out_max[0] = o.out_argmax[0] = buf.ctypes.data
+    fails(L.pb2_beam_peaks(ctypes.byref(o), *[buf.ctypes.data] * 5, None), "dtype")
+    # pulses: invalid parameters are refused at creation; a null chunk at injection
+    edges = np.linspace(400.0, 800.0, 11)
+    var = np.ones(10)
+    p = simpulse._PulseParams(-1.0, 0.0, 1e-3, 0.0, 0.1, 1.0, 10.0, 0.0, 1e9, 1024)
+    h = ctypes.c_void_p()
+    fails(L.pb2_pulse_create(ctypes.byref(p), edges.ctypes.data, var.ctypes.data, 10, ctypes.byref(h)), "dm")
+    p.dm = 50.0
+    assert L.pb2_pulse_create(ctypes.byref(p), edges.ctypes.data, var.ctypes.data, 10, ctypes.byref(h)) == 0
+    fails(L.pb2_pulse_inject(h, None, 0, 10, 256, 256, 0, 1.0, None), "null")
+    fails(L.pb2_pulse_add_to_timestream(h, buf.ctypes.data, 9, 4, 4, 0, 1.0), "row per channel")
+    L.pb2_pulse_destroy(h)
