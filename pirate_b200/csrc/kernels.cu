@@ -37,6 +37,25 @@ template<> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float 
 
 __device__ __forceinline__ float bfly(float x, float y) { return __fmul_rn(kRsqrt2, __fadd_rn(x, y)); }
 
+// Tree butterflies with (NORM) or without the per-step 1/sqrt2. float32 storage normalizes at every
+// step, as the reference does, so that its outputs are bitwise the reference's. 16-bit storage keeps
+// its in-register fp32 sums unnormalized and scales once, by tree_scale(steps) = 2^(-steps/2), where a
+// value leaves the registers (a stored row or an emitted subband): one rounding instead of one per
+// step, and one multiply per stored value instead of one per butterfly.
+template<bool NORM>
+__device__ __forceinline__ float bfly_n(float x, float y) { return NORM ? bfly(x, y) : __fadd_rn(x, y); }
+
+__host__ __device__ constexpr float tree_scale(int steps)
+{
+    float s = (steps & 1) ? kRsqrt2 : 1.0f;
+    for (int i = 0; i < steps / 2; i++) s *= 0.5f;
+    return s;
+}
+
+// A value leaving the registers after n unnormalized butterflies (n is a compile-time constant at
+// every call site once the step loops are unrolled).
+__device__ __forceinline__ float tree_out(float v, int n) { return n ? __fmul_rn(v, tree_scale(n)) : v; }
+
 // Two fp32 additions (multiplications) in one sm_100 packed f32x2 instruction; each element is
 // rounded to nearest like __fadd_rn (__fmul_rn).
 __device__ __forceinline__ unsigned long long f2pack(float2 a)
@@ -523,13 +542,14 @@ template<int K> struct RT
 // needs it) lives in shared memory at *h instead of a register: lane 0 takes it for the lag-1
 // operand, then lane 31 stores this tile's row0. The load precedes the store in the warp's program
 // order, and the loop's __syncwarp() orders the store before the next tile's load.
+template<bool NORM>
 __device__ __forceinline__ void bfly_l0_shared(float &v0, float &v1, float *h, int lane)
 {
     const float x = v0, y = v1, hp = *h;
     float b = __shfl_sync(kFull, x, lane - 1);
     b = (lane == 0) ? hp : b;
-    v0 = bfly(x, y);
-    v1 = bfly(b, y);
+    v0 = bfly_n<NORM>(x, y);
+    v1 = bfly_n<NORM>(b, y);
     if (lane == 31) *h = x;
 }
 
@@ -538,7 +558,8 @@ __device__ __forceinline__ void bfly_l0_shared(float &v0, float &v1, float *h, i
 // (r, q) order), which frees their registers. With EXT0, step 0 (all lags 0) takes its lag-1
 // operands from b0[q] = row 2q one sample earlier, supplied by the caller, and keeps no history;
 // with F0 the caller has already done step 0 itself (from rows it can read one sample earlier).
-template<int K, bool HS = false, bool EXT0 = false, bool F0 = false>
+// NORM: butterflies with the 1/sqrt2 (bfly_n).
+template<int K, bool HS = false, bool EXT0 = false, bool F0 = false, bool NORM = true>
 __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>::NS][RT<K>::NP], int lane, float *hs = nullptr,
                                          const float *b0 = nullptr)
 {
@@ -555,20 +576,20 @@ __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>
                 continue;
             if (EXT0 && r == 0) {
                 const float x = v[i0], y = v[i0 + 1];
-                v[i0] = bfly(x, y);
-                v[i0 + 1] = bfly(b0[q], y);
+                v[i0] = bfly_n<NORM>(x, y);
+                v[i0 + 1] = bfly_n<NORM>(b0[q], y);
                 continue;
             }
             if (HS && L == 0) {
-                bfly_l0_shared(v[i0], v[i0 + h], hs + slot, lane);
+                bfly_l0_shared<NORM>(v[i0], v[i0 + h], hs + slot, lane);
                 slot++;
                 continue;
             }
             float x = v[i0], y = v[i0 + h];
             float a = (L == 0) ? x : lagged(x, pv[r][q], L, lane);
             float b = lagged(x, pv[r][q], L + 1, lane);
-            v[i0] = bfly(a, y);
-            v[i0 + h] = bfly(b, y);
+            v[i0] = bfly_n<NORM>(a, y);
+            v[i0 + h] = bfly_n<NORM>(b, y);
             pv[r][q] = x;
         }
     }
@@ -626,7 +647,9 @@ __device__ __forceinline__ void rt_save(const float (&pv)[RT<K>::NS][RT<K>::NP],
 // (src_lib/ReferenceTree.cpp:120-300): even band pairs coincide with the in-place butterflies, odd
 // ("staggered") pairs (2k+1, 2k+2) are extra butterflies with their own histories ps[r'][u].
 // With F0 the caller has done the level-0 emission and step 0's butterflies (not its emission).
-template<int RB, bool STAG, bool HS, bool EXT0, bool F0, typename Emit>
+// SA: unnormalized butterfly steps the rows have had before phase b (phase a's, or 0); NORM as in
+// rt_steps. Each emitted value is scaled by tree_scale of its unnormalized step count.
+template<int RB, bool STAG, bool HS, bool EXT0, bool F0, int SA, bool NORM, typename Emit>
 __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv)[RT<RB>::NS][RT<RB>::NP],
                                                  float (&ps)[RT<RB>::NS][RT<RB>::NP], const Stage2Args &a,
                                                  int lane, Emit emit, float *hs, const float *b0)
@@ -638,7 +661,7 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
     if (!F0 && a.sb_count[0] > 0) {
 #pragma unroll
         for (int f = 0; f < NB; f++)
-            if (f < a.sb_count[0]) emit(a.sb_mbase[0] + f, v[f]);
+            if (f < a.sb_count[0]) emit(a.sb_mbase[0] + f, tree_out(v[f], SA));
     }
 
 #pragma unroll
@@ -656,8 +679,8 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
                     float aa = (L == 0) ? x : lagged(x, ps[r][u], L, lane);
                     float bb = lagged(x, ps[r][u], L + 1, lane);
                     int m = mb + (2 * k + 1) * (2 << r) + 2 * bitrev_c(j, r);
-                    emit(m, bfly(aa, y));
-                    emit(m + 1, bfly(bb, y));
+                    emit(m, tree_out(bfly_n<NORM>(aa, y), SA + (NORM ? 0 : r + 1)));
+                    emit(m + 1, tree_out(bfly_n<NORM>(bb, y), SA + (NORM ? 0 : r + 1)));
                     ps[r][u] = x;
                 }
             }
@@ -670,17 +693,17 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
                 // done by the caller
             } else if (EXT0 && r == 0) {
                 const float x = v[i0], y = v[i0 + 1];
-                v[i0] = bfly(x, y);
-                v[i0 + 1] = bfly(b0[q], y);
+                v[i0] = bfly_n<NORM>(x, y);
+                v[i0 + 1] = bfly_n<NORM>(b0[q], y);
             } else if (HS && L == 0) {
-                bfly_l0_shared(v[i0], v[i0 + h], hs + slot, lane);
+                bfly_l0_shared<NORM>(v[i0], v[i0 + h], hs + slot, lane);
                 slot++;
             } else {
                 float x = v[i0], y = v[i0 + h];
                 float aa = (L == 0) ? x : lagged(x, pv[r][q], L, lane);
                 float bb = lagged(x, pv[r][q], L + 1, lane);
-                v[i0] = bfly(aa, y);
-                v[i0 + h] = bfly(bb, y);
+                v[i0] = bfly_n<NORM>(aa, y);
+                v[i0 + h] = bfly_n<NORM>(bb, y);
                 pv[r][q] = x;
             }
         }
@@ -692,8 +715,8 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
                 const int k = q >> r, j = q & (h - 1);
                 if (2 * k < cnt) {
                     const int m = mb + (2 * k) * (2 << r) + 2 * bitrev_c(j, r);
-                    emit(m, v[i0]);
-                    emit(m + 1, v[i0 + h]);
+                    emit(m, tree_out(v[i0], SA + (NORM ? 0 : r + 1)));
+                    emit(m + 1, tree_out(v[i0 + h], SA + (NORM ? 0 : r + 1)));
                 }
             }
         }
@@ -897,6 +920,13 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     constexpr bool FA = (STAGE == 2) && (RA >= 1);
     constexpr bool FB = (STAGE == 2) && !STAG && (RB >= 1);
     constexpr bool EB = E0 || FB;
+    // bfly_n per phase: float32 storage normalizes every step. 16-bit storage skips the 1/sqrt2 in both
+    // phases of stage 1 and in phase a of stage 2 (measured 4% and 2% faster), not in stage 2's
+    // phase b (3% slower there), and scales by tree_scale(SU) where values leave the registers.
+    constexpr bool NORM_A = (sizeof(Ts) == 4);
+    constexpr bool NORM_B = (sizeof(Ts) == 4) || (STAGE == 2);
+    constexpr int SA = NORM_A ? 0 : RA;                 // unnormalized steps before phase b
+    constexpr int SU = SA + (NORM_B ? 0 : RB);          // ... and after it
     const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
     float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
 
@@ -1029,15 +1059,15 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                         const Ts *r0 = sb + 2 * q * SPRK + lane + int((offs >> (OB * 2 * q)) & ((1u << OB) - 1));
                         const Ts *r1 = sb + (2 * q + 1) * SPRK + lane + int((offs >> (OB * (2 * q + 1))) & ((1u << OB) - 1));
                         const float xm = to_f(r0[0]), x = to_f(r0[1]), y = to_f(r1[1]);
-                        v[2 * q] = bfly(x, y);
-                        v[2 * q + 1] = bfly(xm, y);
+                        v[2 * q] = bfly_n<NORM_A>(x, y);
+                        v[2 * q + 1] = bfly_n<NORM_A>(xm, y);
                     }
-                    rt_steps<RA, HSA, true, true>(v, pva, lane, hs);
+                    rt_steps<RA, HSA, true, true, NORM_A>(v, pva, lane, hs);
                 } else {
 #pragma unroll
                     for (int i = 0; i < NA; i++)
                         v[i] = to_f(sb[i * SPRK + lane + int((offs >> (OB * i)) & ((1u << OB) - 1))]);
-                    rt_steps<RA, HSA>(v, pva, lane, hs);
+                    rt_steps<RA, HSA, false, false, NORM_A>(v, pva, lane, hs);
                 }
 #pragma unroll
                 for (int i = 0; i < NA; i++)
@@ -1100,11 +1130,11 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                         const int qm = (q0 == lo0) ? (q0 + cap0 - 1) : (q0 - 1);
                         const float x = ring[q0], y = ring[q1], xm = ring[qm];
                         if (STAGE == 2 && cnt0 > 0) {
-                            if (f < cnt0) emit(mb0 + f, x);
-                            if (f + 1 < cnt0) emit(mb0 + f + 1, y);
+                            if (f < cnt0) emit(mb0 + f, tree_out(x, SA));
+                            if (f + 1 < cnt0) emit(mb0 + f + 1, tree_out(y, SA));
                         }
-                        v[f] = bfly(x, y);
-                        v[f + 1] = bfly(xm, y);
+                        v[f] = bfly_n<NORM_B>(x, y);
+                        v[f + 1] = bfly_n<NORM_B>(xm, y);
                     }
                 } else {
 #pragma unroll
@@ -1130,13 +1160,13 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                 }
                 if constexpr (STAGE == 1) {
                     if constexpr (RB >= 1)
-                        rt_steps<RB, HSB, true, true>(v, pvb, lane, hs);
+                        rt_steps<RB, HSB, true, true, NORM_B>(v, pvb, lane, hs);
                     else
-                        rt_steps<RB, HSB, E0>(v, pvb, lane, hs, b0);
+                        rt_steps<RB, HSB, E0, false, NORM_B>(v, pvb, lane, hs, b0);
                     Ts *out = (Ts *) a.ring + (long) bt * a.ring_beam_stride + a.ring_off[(long) blk * NR];
 #pragma unroll
                     for (int f = 0; f < NB; f++)
-                        out[tab_int<NB>(out_base + g * NB, f) + lane] = from_f<Ts>(v[f]);
+                        out[tab_int<NB>(out_base + g * NB, f) + lane] = from_f<Ts>(tree_out(v[f], SU));
                     __syncwarp();
                     if (lane < NB) {
                         const int i = g * NB + lane;
@@ -1144,11 +1174,11 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
                         out_base[i] = (ob == out_off[i] + in_cap[i]) ? out_off[i] : ob;
                     }
                 } else if constexpr (FB) {
-                    phase_b_subbands<RB, STAG, HSB, true, true>(v, pvb, psb, a, lane, emit, hs, b0);
+                    phase_b_subbands<RB, STAG, HSB, true, true, SA, NORM_B>(v, pvb, psb, a, lane, emit, hs, b0);
                 } else {
                     emit.row0 = pf_rows + pf_slot;
                     pf_slot = (pf_slot + 32) & int(a.pf_cap - 1);
-                    phase_b_subbands<RB, STAG, HSB, E0, false>(v, pvb, psb, a, lane, emit, hs, b0);
+                    phase_b_subbands<RB, STAG, HSB, E0, false, SA, NORM_B>(v, pvb, psb, a, lane, emit, hs, b0);
                 }
             }
             asm volatile("bar.sync 1, %0;" :: "r"(blockDim.x) : "memory");
