@@ -930,9 +930,19 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
     float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
 
+    // The shared delay line comes back from HBM with 16-byte cp.async copies (RING is a multiple of 32
+    // floats, and each block's state starts on a 16-byte boundary), overlapping the table setup below;
+    // each thread waits for its copies before the block barrier that ends the setup.
+    const bool st16 = ((reinterpret_cast<uintptr_t>(st) & 15) == 0);
+    if (st16) {
+        for (int i = threadIdx.x; i < RING / 4; i += blockDim.x)
+            cp_async_bytes<16>(ring + 4 * i, st + 4 * i);
+        cp_async_commit();
+    } else {
+        for (int i = threadIdx.x; i < RING; i += blockDim.x)
+            ring[i] = st[i];
+    }
     ring_init<RA, RB>(wb, rt, in_cap, a.s0);
-    for (int i = threadIdx.x; i < RING; i += blockDim.x)
-        ring[i] = st[i];
 
     const Ts *in;
     int pos1 = 0;   // stage 1: read position of every input row (rows are read aligned)
@@ -964,6 +974,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     const bool is_a = warp < NB;
     const int g = is_a ? warp : (warp - NB);   // phase-a group (f) or phase-b group (d)
     const int ntiles = a.nt / 32;
+    cp_async_wait0();
     __syncthreads();
     // Register splits between the warp roles (whole warpgroups: phase a is warps 0-15). Each block is
     // launched with the kernel's allocation, and the split adds up to exactly that, so the increasing
@@ -1188,8 +1199,13 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     }
     __syncthreads();
 
-    for (int i = threadIdx.x; i < RING; i += blockDim.x)
-        st[i] = ring[i];
+    if (st16) {
+        for (int i = threadIdx.x; i < RING / 4; i += blockDim.x)
+            reinterpret_cast<float4 *>(st)[i] = reinterpret_cast<const float4 *>(ring)[i];
+    } else {
+        for (int i = threadIdx.x; i < RING; i += blockDim.x)
+            st[i] = ring[i];
+    }
 }
 
 

@@ -116,8 +116,10 @@ struct GridLdsArgs
 };
 
 // Floats of persistent state per block of the stage kernels (host and device agree by construction).
-inline long stage1_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), false); }
-inline long stage2_state_floats(int R) { return tree_state_floats(split_ra(R), split_rb(R), true); }
+// Per-block state, rounded up to a multiple of 4 floats so that every block's state starts on a
+// 16-byte boundary (the kernels move its delay-line part with 16-byte copies).
+inline long stage1_state_floats(int R) { return (tree_state_floats(split_ra(R), split_rb(R), false) + 3) & ~3L; }
+inline long stage2_state_floats(int R) { return (tree_state_floats(split_ra(R), split_rb(R), true) + 3) & ~3L; }
 
 // Per-beam peak of a batch's outputs, as pirate's toy grouper reduces them (pirate_frb/run_toy_grouper.py:
 // 79-116): over every tree, the maximum of out_max[tree][b] and its first (dm, time) position; a tree
