@@ -106,7 +106,27 @@ void GpuDedisperser::stop(std::exception_ptr e)
 
 int GpuDedisperser::kernels_per_batch() const
 {
-    return 1 + int(plan.num_primary_trees) + 2 * int(plan.ntrees);
+    return 1 + int(plan.num_primary_trees) + stage2_launches() + int(plan.ntrees);
+}
+
+// Stage-2 launches per batch: runs of consecutive output trees with the same stage-2 kernel (same dd
+// rank and staggered-subband flag), at most kStage2MaxTrees per launch.
+int GpuDedisperser::stage2_launches() const
+{
+    int n = 0;
+    for (long i0 = 0; i0 < plan.ntrees;) {
+        long i1 = i0 + 1;
+        auto stag = [&](long i) {
+            const FrequencySubbands &fs = plan.trees[i].frequency_subbands;
+            bool x = false;
+            for (long l = 1; l <= fs.pf_rank && l < 5; l++) x = x || (fs.subband_counts[l] >= 2);
+            return x;
+        };
+        while (i1 < plan.ntrees && i1 - i0 < kStage2MaxTrees && plan.trees[i1].dd_rank == plan.trees[i0].dd_rank && stag(i1) == stag(i0)) i1++;
+        n++;
+        i0 = i1;
+    }
+    return n;
 }
 
 std::vector<double> GpuDedisperser::algorithmic_bytes() const
@@ -433,11 +453,13 @@ void GpuDedisperser::launch_batch(long seq_id)
         tick(2, t2);
     }
 
+    std::vector<Stage2Args> a2(plan.ntrees);
+    std::vector<int> nb2(plan.ntrees);
     for (long i = 0; i < plan.ntrees; i++) {
         const DedispersionTree &t = plan.trees[i];
         Stage2 &st = s2[i];
         Stage1 &src = s1[t.primary_tree_index];
-        Stage2Args a;
+        Stage2Args &a = a2[i];
         memset(&a, 0, sizeof(a));
         a.rank = t.dd_rank;
         a.state_per_block = st.state_per_block;
@@ -456,9 +478,16 @@ void GpuDedisperser::launch_batch(long seq_id)
         a.s0 = ichunk * t.nt_ds;
         a.nt = t.nt_ds;
         a.beam0 = beam0;
+        nb2[i] = int(st.nblocks);
+    }
+    // Consecutive output trees that use the same stage-2 kernel share one launch.
+    for (long i0 = 0; i0 < plan.ntrees;) {
+        long i1 = i0 + 1;
+        while (i1 < plan.ntrees && i1 - i0 < kStage2MaxTrees && stage2_same_kernel(a2[i0], a2[i1])) i1++;
         cudaEvent_t t3 = tick(3, nullptr);
-        launch_stage2(a, dtype_code, st.nblocks, int(B), s);
+        launch_stage2_multi(&a2[i0], &nb2[i0], int(i1 - i0), dtype_code, int(B), s);
         tick(3, t3);
+        i0 = i1;
     }
 
     // Output back-pressure: slot_out is reusable once every consumer released seq_id - nbatches_out.

@@ -88,6 +88,7 @@ public:
     size_t device_bytes() const { return total_bytes; }
     // Number of kernels launched per (chunk, batch).
     int kernels_per_batch() const;
+    int stage2_launches() const;
     // Bytes of HBM traffic per (chunk, batch) of each kernel class (algorithmic):
     // [grid+lds (one fused kernel), unused, stage1, stage2, pf].
     std::vector<double> algorithmic_bytes() const;

@@ -17,6 +17,7 @@
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -884,13 +885,34 @@ struct TreeArgsOf;
 template<> struct TreeArgsOf<1> { using type = Stage1Args; };
 template<> struct TreeArgsOf<2> { using type = Stage2Args; };
 
+// Launch parameter: one stage-1 tree, or a grid of stage-2 trees (Stage2Multi).
+template<int STAGE>
+struct TreeParamOf;
+template<> struct TreeParamOf<1> { using type = Stage1Args; };
+template<> struct TreeParamOf<2> { using type = Stage2Multi; };
+
+template<int STAGE, typename PT>
+__device__ __forceinline__ const typename TreeArgsOf<STAGE>::type &tree_args(const PT &P, int ti)
+{
+    if constexpr (STAGE == 1) return P;
+    else return P.t[ti];
+}
+
 // Two-phase tree kernel. Warps [0, NB) run phase a on tile k while warps [NB, NB+NA) run phase b on
 // tile k-1; one block barrier per tile.
 //   STAGE 1: input = level-p tree rows (aligned), output = per-row stage-1 delay lines.
 //   STAGE 2: input = stage-1 delay lines read at lag rb_lag (misaligned), output = subband rows.
 template<typename Ts, int RA, int RB, int STAGE, bool STAG, bool HS = tree_hs(RA, RB, STAGE)>
-__global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(typename TreeArgsOf<STAGE>::type a)
+__global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(const __grid_constant__ typename TreeParamOf<STAGE>::type P)
 {
+    // Stage 2: this block's tree ti and its block index blk among that tree's nblk blocks.
+    int ti = 0, blk = blockIdx.x, nblk = gridDim.x;
+    if constexpr (STAGE == 2) {
+        while (ti + 1 < P.n && blk >= P.blk0[ti + 1]) ti++;
+        nblk = P.blk0[ti + 1] - P.blk0[ti];
+        blk -= P.blk0[ti];
+    }
+    const auto &a = tree_args<STAGE>(P, ti);
     constexpr int NA = 1 << RA, NB = 1 << RB, NR = 1 << (RA + RB);
     constexpr int RING = ring_floats(RA, RB);
     // Staging row stride: stage-1 rows are 32 aligned samples; stage-2 rows take one more chunk.
@@ -927,8 +949,8 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(t
     constexpr bool NORM_B = (sizeof(Ts) == 4) || (STAGE == 2);
     constexpr int SA = NORM_A ? 0 : RA;                 // unnormalized steps before phase b
     constexpr int SU = SA + (NORM_B ? 0 : RB);          // ... and after it
-    const int blk = blockIdx.x, b = blockIdx.y, bt = a.beam0 + b;
-    float *st = a.state + ((long) bt * gridDim.x + blk) * a.state_per_block;
+    const int b = blockIdx.y, bt = a.beam0 + b;
+    float *st = a.state + ((long) bt * nblk + blk) * a.state_per_block;
 
     // The shared delay line comes back from HBM with 16-byte cp.async copies (RING is a multiple of 32
     // floats, and each block's state starts on a 16-byte boundary), overlapping the table setup below;
@@ -1888,9 +1910,9 @@ static void launch_tree_r(const A &a, int nblocks, int B, cudaStream_t s)
 }
 
 template<typename Ts, int STAGE, bool STAG, typename A>
-static void launch_tree_t(const A &a, int nblocks, int B, cudaStream_t s)
+static void launch_tree_t(const A &a, int rank, int nblocks, int B, cudaStream_t s)
 {
-    switch (a.rank) {
+    switch (rank) {
     case 1: launch_tree_r<Ts, 1, STAGE, STAG>(a, nblocks, B, s); break;
     case 2: launch_tree_r<Ts, 2, STAGE, STAG>(a, nblocks, B, s); break;
     case 3: launch_tree_r<Ts, 3, STAGE, STAG>(a, nblocks, B, s); break;
@@ -1899,31 +1921,60 @@ static void launch_tree_t(const A &a, int nblocks, int B, cudaStream_t s)
     case 6: launch_tree_r<Ts, 6, STAGE, STAG>(a, nblocks, B, s); break;
     case 7: launch_tree_r<Ts, 7, STAGE, STAG>(a, nblocks, B, s); break;
     case 8: launch_tree_r<Ts, 8, STAGE, STAG>(a, nblocks, B, s); break;
-    default: throw std::runtime_error("tree_kernel: unsupported dd rank " + std::to_string(a.rank));
+    default: throw std::runtime_error("tree_kernel: unsupported dd rank " + std::to_string(rank));
     }
 }
 
 void launch_stage1(const Stage1Args &a, int dtype, int nblocks, int B, cudaStream_t s)
 {
     if (a.in_lag0 != 0 || a.in_lag1 != 0) throw std::runtime_error("launch_stage1: input rows must be aligned (no read lag)");
-    if (dtype == 0) launch_tree_t<float, 1, false>(a, nblocks, B, s);
-    else if (dtype == 1) launch_tree_t<__half, 1, false>(a, nblocks, B, s);
-    else launch_tree_t<__nv_bfloat16, 1, false>(a, nblocks, B, s);
+    if (dtype == 0) launch_tree_t<float, 1, false>(a, a.rank, nblocks, B, s);
+    else if (dtype == 1) launch_tree_t<__half, 1, false>(a, a.rank, nblocks, B, s);
+    else launch_tree_t<__nv_bfloat16, 1, false>(a, a.rank, nblocks, B, s);
+}
+
+static bool stage2_staggered(const Stage2Args &a)
+{
+    bool stag = false;
+    for (int l = 1; l < 5; l++) stag = stag || (a.sb_count[l] >= 2);
+    return stag;
+}
+
+bool stage2_same_kernel(const Stage2Args &x, const Stage2Args &y)
+{
+    return x.rank == y.rank && stage2_staggered(x) == stage2_staggered(y);
+}
+
+void launch_stage2_multi(const Stage2Args *a, const int *nblocks, int n, int dtype, int B, cudaStream_t s)
+{
+    if (n < 1 || n > kStage2MaxTrees) throw std::runtime_error("launch_stage2_multi: bad tree count " + std::to_string(n));
+    Stage2Multi m;
+    memset(&m, 0, sizeof(m));
+    m.n = n;
+    long tot = 0;
+    for (int i = 0; i < n; i++) {
+        if (!stage2_same_kernel(a[0], a[i])) throw std::runtime_error("launch_stage2_multi: trees need different kernels");
+        if (nblocks[i] < 1) throw std::runtime_error("launch_stage2_multi: bad block count");
+        m.t[i] = a[i];
+        m.blk0[i] = int(tot);
+        tot += nblocks[i];
+    }
+    if (tot > (1L << 30)) throw std::runtime_error("launch_stage2_multi: grid too large");
+    m.blk0[n] = int(tot);
+    if (stage2_staggered(a[0])) {
+        if (dtype == 0) launch_tree_t<float, 2, true>(m, a[0].rank, int(tot), B, s);
+        else if (dtype == 1) launch_tree_t<__half, 2, true>(m, a[0].rank, int(tot), B, s);
+        else launch_tree_t<__nv_bfloat16, 2, true>(m, a[0].rank, int(tot), B, s);
+    } else {
+        if (dtype == 0) launch_tree_t<float, 2, false>(m, a[0].rank, int(tot), B, s);
+        else if (dtype == 1) launch_tree_t<__half, 2, false>(m, a[0].rank, int(tot), B, s);
+        else launch_tree_t<__nv_bfloat16, 2, false>(m, a[0].rank, int(tot), B, s);
+    }
 }
 
 void launch_stage2(const Stage2Args &a, int dtype, int nblocks, int B, cudaStream_t s)
 {
-    bool stag = false;
-    for (int l = 1; l < 5; l++) stag = stag || (a.sb_count[l] >= 2);
-    if (stag) {
-        if (dtype == 0) launch_tree_t<float, 2, true>(a, nblocks, B, s);
-        else if (dtype == 1) launch_tree_t<__half, 2, true>(a, nblocks, B, s);
-        else launch_tree_t<__nv_bfloat16, 2, true>(a, nblocks, B, s);
-    } else {
-        if (dtype == 0) launch_tree_t<float, 2, false>(a, nblocks, B, s);
-        else if (dtype == 1) launch_tree_t<__half, 2, false>(a, nblocks, B, s);
-        else launch_tree_t<__nv_bfloat16, 2, false>(a, nblocks, B, s);
-    }
+    launch_stage2_multi(&a, &nblocks, 1, dtype, B, s);
 }
 
 int pf_warp_floats(int Dout, int tpad, int Dcore, int L)

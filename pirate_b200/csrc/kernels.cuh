@@ -151,6 +151,19 @@ void launch_dequantize(void *out, int out_dtype, const void *data, const void *s
                        long ntime, cudaStream_t s);
 void launch_stage1(const Stage1Args &a, int dtype, int nblocks, int B, cudaStream_t s);
 void launch_stage2(const Stage2Args &a, int dtype, int nblocks, int B, cudaStream_t s);
+
+// Stage 2 of several output trees that use the same kernel (same dd rank and staggered-subband flag)
+// as one grid: blocks [blk0[i], blk0[i+1]) are tree i's. One grid has one partial last wave instead of
+// one per tree (the downsampled trees' grids are 3.5 waves).
+constexpr int kStage2MaxTrees = 8;
+struct Stage2Multi
+{
+    Stage2Args t[kStage2MaxTrees];
+    int blk0[kStage2MaxTrees + 1];
+    int n;
+};
+bool stage2_same_kernel(const Stage2Args &x, const Stage2Args &y);
+void launch_stage2_multi(const Stage2Args *a, const int *nblocks, int n, int dtype, int B, cudaStream_t s);
 void launch_pf(const PfArgs &a, int dtype, int B, cudaStream_t s);
 
 struct DedispersionPlan;
