@@ -173,3 +173,25 @@ def test_new_entry_points_validate_arguments(pb2lib):
     fails(L.pb2_pulse_inject(h, None, 0, 10, 256, 256, 0, 1.0, None), "null")
     fails(L.pb2_pulse_add_to_timestream(h, buf.ctypes.data, 9, 4, 4, 0, 1.0), "row per channel")
     L.pb2_pulse_destroy(h)
+
+
+def test_kernel_launches_per_batch(pb2lib):
+    """Launch count per (chunk, batch), from the plan alone (no GPU needed): gridding, one stage-1
+    launch per primary tree, one stage-2 grid per run of consecutive output trees that share a stage-2
+    kernel (same dd rank and staggered-subband flag), one peak-finding launch per output tree."""
+    prim = [dict(num_early_triggers=0, max_width=32, dm_downsampling=0, time_downsampling=0,
+                 wt_dm_downsampling=64, wt_time_downsampling=64) for _ in range(5)]
+    cfg = H.toy_config(rank=16, nfreq=16384, nt=2048, dtype="float16", subbands=[0, 0, 0, 0, 1], beams_per_gpu=4,
+                       beams_per_batch=4, primary_trees=prim)
+    plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(cfg))
+    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=1)
+    # the benchmark's plan: its five output trees share one stage-2 kernel (dd rank 8, no staggered pairs)
+    assert plan.ntrees == 5 and {t.dd_rank for t in plan.trees} == {8}
+    assert dd.kernels_per_batch() == 1 + 5 + 1 + 5
+    # plans with early triggers and subbands: between one stage-2 grid and one per output tree
+    for case in ([2, 2, 1], [1, 1, 1], [0, 1]):
+        cfg = H.toy_config(rank=9, nfreq=300, nt=256, subbands=case)
+        plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(cfg))
+        n = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=1).kernels_per_batch()
+        npri = len(cfg["primary_trees"])
+        assert 1 + npri + 1 + plan.ntrees <= n <= 1 + npri + 2 * plan.ntrees, (case, n)
