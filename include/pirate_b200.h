@@ -223,7 +223,10 @@ void pb2_dd_destroy(pb2_dedisperser *dd);
  *   out_max[i], out_argmax[i]: device (beams_per_batch, ndm_out, nt_out), config dtype / uint32
  * The array is shared by all calls: calls that overlap on the GPU race and must be serialized.
  * The first call on a device looks up the array's address (cudaGetSymbolAddress); make that first
- * call before any stream capture. */
+ * call before any stream capture. The stream must belong to the current device. The plan's lookup
+ * tables are copied from pageable host memory on the first call on a device and whenever the plan
+ * differs from the previous call's, so such a call may wait for earlier work on the stream; calls
+ * that repeat the previous plan copy nothing from the host. */
 #define PB2_NOALLOC_SCRATCH_BYTES (32L << 20)
 int pb2_dedisperse_chunk_noalloc(const pb2_plan *plan, const void *in, const float *const *weights,
                                  void *const *out_max, uint32_t *const *out_argmax, void *stream);

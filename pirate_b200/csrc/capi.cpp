@@ -507,6 +507,9 @@ int pb2_dedisperse_chunk_noalloc(const pb2_plan *plan, const void *in, const flo
 {
     return guard([&] {
         REQUIRE_PTR(plan); REQUIRE_PTR(in); REQUIRE_PTR(weights); REQUIRE_PTR(out_max); REQUIRE_PTR(out_argmax);
+        for (long i = 0; i < plan->p->ntrees; i++) {
+            REQUIRE_PTR(weights[i]); REQUIRE_PTR(out_max[i]); REQUIRE_PTR(out_argmax[i]);
+        }
         pb2::dedisperse_chunk_noalloc(*plan->p, in, weights, out_max, out_argmax, (cudaStream_t) stream);
     });
 }

@@ -89,7 +89,8 @@ public:
     // Number of kernels launched per (chunk, batch).
     int kernels_per_batch() const;
     int stage2_launches() const;
-    // Bytes of HBM traffic per (chunk, batch) of each kernel class (algorithmic):
+    // Bytes of HBM traffic per (chunk, batch) of each kernel class (algorithmic: each element read or
+    // written once, following pirate's ResourceTracker model):
     // [grid+lds (one fused kernel), unused, stage1, stage2, pf].
     std::vector<double> algorithmic_bytes() const;
 

@@ -16,7 +16,13 @@
 //
 // On the first call on a device, the address of the array on that device is looked up with
 // cudaGetSymbolAddress() (with that device current) and cached. That first call should come
-// before any stream capture.
+// before any stream capture. The stream must belong to the current device.
+//
+// Lookup tables. The plan's tables (channel weights, delay-line offsets) sit at the start of the
+// array. A call uploads them only when its tables differ from the last ones uploaded on this device,
+// i.e. on the first call and whenever the plan changes; the copy is then from pageable host memory,
+// so that call may wait for earlier work on its stream. Calls that repeat the previous plan copy
+// nothing from the host: they clear the rest of the array and launch the kernels.
 
 #include "../../include/pirate_b200.h"
 #include "kernels.cuh"
@@ -42,14 +48,13 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 static long na_pow2_ceil(long n) { long p = 1; while (p < n) p <<= 1; return p; }
 static long na_round_up(long n, long k) { return ((n + k - 1) / k) * k; }
 
+static std::mutex g_noalloc_mtx;
+
 // Scratch address of the current device (looked up once per device).
-static unsigned char *noalloc_scratch()
+static unsigned char *noalloc_scratch(int dev)
 {
-    static std::mutex mtx;
     static std::vector<unsigned char *> addr;
-    int dev = 0;
-    NA_CHECK(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mtx);
+    std::lock_guard<std::mutex> lk(g_noalloc_mtx);
     if ((int) addr.size() <= dev) addr.resize(dev + 1, nullptr);
     if (!addr[dev]) {
         void *p = nullptr;
@@ -144,6 +149,8 @@ void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, cons
         const DedispersionTree &t = plan.trees[i];
         const FrequencySubbands &fs = t.frequency_subbands;
         if (t.dd_rank < 1 || t.dd_rank > 8) throw std::runtime_error("pb2_dedisperse_chunk_noalloc: stage-2 dd rank must be in [1, 8]");
+        if (fs.pf_rank != split_rb(t.dd_rank) || fs.pf_rank < 0 || fs.pf_rank >= 5)
+            throw std::runtime_error("pb2_dedisperse_chunk_noalloc: unexpected peak-finding rank");
         S2 &st = s2[i];
         st.M = int(fs.M);
         st.N = int(fs.N);
@@ -155,6 +162,7 @@ void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, cons
         int mb = 0;
         for (int l = 0; l < 5; l++) { st.cnt[l] = 0; st.mb[l] = 0; }
         for (int l = 0; l <= fs.pf_rank; l++) { st.cnt[l] = int(fs.subband_counts[l]); st.mb[l] = mb; mb += int(fs.subband_counts[l]) << l; }
+        if (mb != st.M) throw std::runtime_error("pb2_dedisperse_chunk_noalloc: multiplet count mismatch");
         std::vector<int> m2n(st.M);
         for (int m = 0; m < st.M; m++) m2n[m] = int(fs.m_to_n[m]);
         st.m2n_t = tab.put(m2n.data(), st.M * sizeof(int));
@@ -185,9 +193,27 @@ void dedisperse_chunk_noalloc(const DedispersionPlan &plan, const void *in, cons
         throw std::runtime_error(ss.str());
     }
 
-    unsigned char *base = noalloc_scratch();
+    int dev = 0;
+    NA_CHECK(cudaGetDevice(&dev));
+    if (stream) {
+        int sdev = -1;
+        NA_CHECK(cudaStreamGetDevice(stream, &sdev));
+        if (sdev != dev)
+            throw std::runtime_error("pb2_dedisperse_chunk_noalloc: the stream belongs to another device than the current one");
+    }
+    unsigned char *base = noalloc_scratch(dev);
+    {
+        // Upload the tables only if they differ from the last ones uploaded on this device.
+        static std::vector<std::vector<unsigned char>> last;
+        std::lock_guard<std::mutex> lk(g_noalloc_mtx);
+        if ((int) last.size() <= dev) last.resize(dev + 1);
+        if (last[dev] != tab.bytes) {
+            last[dev].clear();   // a failed upload leaves no stale record
+            NA_CHECK(cudaMemcpyAsync(base + tab_at, tab.bytes.data(), tab.bytes.size(), cudaMemcpyHostToDevice, stream));
+            last[dev] = tab.bytes;
+        }
+    }
     NA_CHECK(cudaMemsetAsync(base + zero_from, 0, cv.used - zero_from, stream));
-    NA_CHECK(cudaMemcpyAsync(base + tab_at, tab.bytes.data(), tab.bytes.size(), cudaMemcpyHostToDevice, stream));
     auto T = [&](long o) { return base + tab_at + o; };
     auto P = [&](long o) { return base + o; };
 

@@ -3,7 +3,7 @@
 sample of them on the benchmark's full rank-16 plan, as fixtures for pirate_b200.PfAvarApproximation
 and GpuDedisperser.fill_analytic_weights.
 
-    python tests/golden/make_avar_golden.py [PIRATE_SRC]      (default PIRATE_SRC: /root/reference)
+    python tests/golden/make_avar_golden.py PIRATE_SRC      (the pirate source tree, required)
 
 pirate's python package cannot be imported as a whole here (its compiled extension is not built), so
 the two pure-numpy modules are loaded from their files with small stand-ins for the two names they
@@ -106,7 +106,9 @@ def full_freq_variances(nfreq):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_avar_golden.py PIRATE_SRC")
+    src = sys.argv[1]
     PV = load_slow_avar(src)
     rng = np.random.default_rng(2024)
     out = {}

@@ -1,7 +1,7 @@
 """Generates the committed golden fixtures of tests/golden. Run in a checkout that has pirate's
-source tree available (its path is the first argument, default /root/reference):
+source tree available (its path is the required first argument):
 
-    python tests/golden/make_golden.py [PIRATE_SRC]
+    python tests/golden/make_golden.py PIRATE_SRC
 
   example_plan_trees.json  config + per-tree plan fields of pirate's configs/example_dedispersion_plan.yml
                            (the plan pirate's own 'show_dedisperser' printed for configs/dedispersion/chord_sb2_et.yml)
@@ -59,7 +59,9 @@ def toy():
 
 
 if __name__ == "__main__":
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py PIRATE_SRC")
+    src = sys.argv[1]
     example_plan(src)
     toy()
     print("wrote", os.listdir(HERE))

@@ -31,24 +31,30 @@ def _noalloc(pb, plan, x, ws, outs_max, outs_arg, stream):
     return f(plan._h, x.data_ptr(), wp, mp, ap, stream.cuda_stream)
 
 
-def test_noalloc_matches_gpu_dedisperser(pb2lib):
+@pytest.mark.parametrize("dtype,beams", [("float32", 1), ("float16", 2)])
+def test_noalloc_matches_gpu_dedisperser(pb2lib, dtype, beams):
+    """float32 with one beam, and float16 (the benchmark's storage) with two beams per batch, so that
+    the per-beam strides of every scratch region are exercised. Both entry points run the same kernels
+    on the same inputs, so even float16 outputs must agree bit for bit."""
     import torch
     pb = pb2lib
-    cfg = H.toy_config(rank=8, nfreq=640, nt=256, subbands=[2, 2, 1], beams_per_gpu=1, beams_per_batch=1)
+    cfg = H.toy_config(rank=8, nfreq=640, nt=256, dtype=dtype, subbands=[2, 2, 1], beams_per_gpu=beams,
+                       beams_per_batch=beams)
     plan = pb.DedispersionPlan(pb.DedispersionConfig.from_dict(cfg))
     orc, _ = H.run_oracle(cfg, [], [])
     ws_host = H.make_weights(orc, seed=5)
     dev = torch.device("cuda:0")
     stream = torch.cuda.current_stream()
     ws_dev = [torch.from_numpy(w[0]).to(dev) for w in ws_host]
-    outs_max = [torch.empty(orc.out_shape(i), dtype=torch.float32, device=dev) for i in range(plan.ntrees)]
+    tdt = getattr(torch, dtype)
+    outs_max = [torch.empty(orc.out_shape(i), dtype=tdt, device=dev) for i in range(plan.ntrees)]
     outs_arg = [torch.empty(orc.out_shape(i), dtype=torch.int32, device=dev) for i in range(plan.ntrees)]
 
     for call in range(2):
         x = H.make_inputs(cfg, 1, seed=100 + call)[0]
         # Existing entry points: chunk 0 of a fresh GpuDedisperser.
         _, _, ref = H.run_gpu(pb, cfg, [x], ws_host)
-        xd = torch.from_numpy(x).to(dev)
+        xd = torch.from_numpy(x).to(dev).to(tdt)
         for m, a in zip(outs_max, outs_arg):
             m.fill_(123.0)
             a.fill_(-7)
