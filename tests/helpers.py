@@ -23,6 +23,33 @@ def toy_config(rank=8, nfreq=640, nt=256, dtype="float32", subbands=(2, 2, 1), b
                 num_active_batches=num_active_batches, future_write_max_samples=0, max_gpu_clag=10000)
 
 
+# (rank, nfreq, nt, subbands, primary trees as (num_early_triggers, max_width), beams_per_gpu, beams_per_batch)
+PARITY_CASES = [
+    (6, 100, 128, [1], [(0, 4)], 1, 1),
+    (8, 640, 256, [2, 2, 1], [(0, 16), (1, 8)], 2, 1),
+    (9, 300, 256, [1, 1, 1], [(1, 32), (0, 8), (1, 2)], 2, 2),
+    (10, 1024, 512, [0, 0, 1], [(0, 32), (0, 16), (0, 8)], 1, 1),
+    (11, 2000, 256, [3, 5, 3, 1], [(2, 8), (1, 4)], 4, 2),
+    (7, 50, 128, [1, 1], [(0, 1), (0, 2)], 3, 1),
+    # explicit output time downsampling (third entry): 16 and 32 (saturated boxcar levels, partial
+    # 32-output tiles), 64, 2 and 1
+    (8, 256, 512, [0, 1, 1], [(0, 32, 16), (0, 16, 32)], 2, 1),
+    (7, 128, 512, [1, 1], [(0, 8, 64), (0, 4, 2), (0, 2, 1)], 1, 1),
+]
+
+
+def case_config(case, dtype="float32"):
+    rank, nfreq, nt, sb, pts, bpg, bpb = case
+    prim = []
+    for ip, pt in enumerate(pts):
+        net, w = pt[:2]
+        tds = pt[2] if len(pt) > 2 else 0
+        prim.append(dict(num_early_triggers=net, max_width=w, dm_downsampling=0, time_downsampling=tds,
+                         wt_dm_downsampling=2 ** ((rank - (1 if ip else 0) - net) // 2), wt_time_downsampling=max(16, tds)))
+    return toy_config(rank=rank, nfreq=nfreq, nt=nt, dtype=dtype, subbands=sb, beams_per_gpu=bpg,
+                      beams_per_batch=bpb, num_active_batches=1, primary_trees=prim)
+
+
 def quantize(x, dtype):
     """Rounds float32 data to the storage dtype and back (what the GPU path sees)."""
     import torch
@@ -88,3 +115,99 @@ def run_oracle(cfg, xs, weights, sophistication=1, real_bits=32, keep=None):
         extra = keep(orc, seq) if keep else None
         res.append((m, a, extra))
     return orc, res
+
+
+# ---- Fixture cases pinned to pirate's own reference dedisperser (tests/golden/make_ref_golden.py) ----
+
+def _prim(rank, pts, wt_time=16):
+    prim = []
+    for ip, (net, w, tds) in enumerate(pts):
+        prim.append(dict(num_early_triggers=net, max_width=w, dm_downsampling=0, time_downsampling=tds,
+                         wt_dm_downsampling=2 ** ((rank - (1 if ip else 0) - net) // 2),
+                         wt_time_downsampling=max(wt_time, tds)))
+    return prim
+
+
+def pirate_fixture_cases():
+    """Cases whose outputs from pirate's ReferenceDedisperser are committed as fixtures. Each entry:
+    name, cfg, nchunks, input seed, weight seed, weight kind ('random' or 'bare'), extras."""
+    cases = []
+    for k, c in enumerate(PARITY_CASES):
+        cases.append(dict(name="parity%d_r%d" % (k, c[0]), cfg=case_config(c), nchunks=5,
+                          seed=c[0] * 7 + c[2], wseed=c[0], wkind="random", extra=None))
+    cases.append(dict(name="nan_r8", cfg=case_config(PARITY_CASES[1]), nchunks=3, seed=5, wseed=2,
+                      wkind="random", extra="nan"))
+    # The reference's own CPU-runnable case: rank 10 from 1024 channels, one tree, widths 1-8, no
+    # subbands, 4 chunks of 2048 samples, one dispersed boxcar pulse (width 4, amplitude 1 per channel).
+    cases.append(dict(name="rank10_pulse", cfg=toy_config(rank=10, nfreq=1024, nt=2048, subbands=[0, 0, 0, 1],
+                                                         beams_per_gpu=1, beams_per_batch=1,
+                                                         primary_trees=_prim(10, [(0, 8, 0)], 64)),
+                      nchunks=4, seed=1010, wseed=0, wkind="bare", extra="pulse"))
+    # Five primary trees at rank 12, run until the longest delay lines of every tree have wrapped
+    # (tree 4's longest lag is 2^11 samples of 16-fold downsampled time, 64 chunks of 512).
+    cases.append(dict(name="rank12_5trees_wrap", cfg=toy_config(rank=12, nfreq=2048, nt=512, subbands=[0, 0, 0, 0, 1],
+                                                               beams_per_gpu=1, beams_per_batch=1,
+                                                               primary_trees=_prim(12, [(0, 32, 0)] * 5, 16)),
+                      nchunks=68, seed=1212, wseed=12, wkind="random", extra=None))
+    # Rank 16 (stage ranks 8 + 8) with an early trigger, two chunks.
+    cases.append(dict(name="rank16_et", cfg=toy_config(rank=16, nfreq=4096, nt=2048, subbands=[0, 2, 0, 0, 1],
+                                                      beams_per_gpu=1, beams_per_batch=1,
+                                                      primary_trees=_prim(16, [(1, 32, 0)], 64)),
+                      nchunks=2, seed=16, wseed=16, wkind="random", extra=None))
+    # Rank 16, one primary tree, 34 chunks of 2048: the longest stage-1 -> stage-2 delay lines (2^16
+    # samples, 32 chunks) wrap inside the compared run. Compared on the GPU only (the CPU oracle needs
+    # minutes for it).
+    cases.append(dict(name="rank16_wrap", cfg=toy_config(rank=16, nfreq=4096, nt=2048, subbands=[0, 0, 0, 0, 1],
+                                                        beams_per_gpu=1, beams_per_batch=1,
+                                                        primary_trees=_prim(16, [(0, 32, 0)], 64)),
+                      nchunks=34, seed=1616, wseed=17, wkind="random", extra=None, cpu=False))
+    return cases
+
+
+def fixture_inputs(case):
+    """The seeded inputs of a fixture case, in seq_id order (float32, exactly representable in the
+    case's storage dtype)."""
+    cfg = case["cfg"]
+    xs = make_inputs(cfg, case["nchunks"], seed=case["seed"])
+    if case["extra"] == "nan":
+        rng = np.random.default_rng(17)
+        for x in xs:
+            x[rng.random(x.shape) < 2e-4] = np.nan
+        nb = cfg["beams_per_gpu"] // cfg["beams_per_batch"]
+        xs[nb][:, :, 100:104] = np.nan
+    elif case["extra"] == "pulse":
+        # Dispersed boxcar: arrival t0 + k_DM * DM * (nu^-2 - nu_hi^-2) per channel (k_DM = 4.148806e6
+        # ms MHz^2 cm^3 / pc), DM = 30 pc/cm^3, inside tree 0's range (full-band delay 583 of 1024 samples).
+        F = sum(cfg["zone_nfreq"])
+        T = cfg["time_samples_per_chunk"]
+        lo, hi = cfg["zone_freq_edges"][0], cfg["zone_freq_edges"][-1]
+        nu = lo + (np.arange(F) + 0.5) * (hi - lo) / F
+        delay_ms = 4.148806e6 * 30.0 * (nu ** -2 - hi ** -2)
+        t0 = 3000
+        full = np.concatenate(xs, axis=2)   # (B, F, nchunks*T)
+        for f in range(F):
+            a = t0 + int(round(delay_ms[f] / cfg["time_sample_ms"]))
+            full[:, f, a:a + 4] += 1.0
+        xs = [np.ascontiguousarray(full[:, :, c * T:(c + 1) * T]) for c in range(case["nchunks"])]
+    return xs
+
+
+def fixture_weights(case, orc):
+    return make_weights(orc, seed=case["wseed"], kind=case["wkind"])
+
+
+def output_digest(out_max, out_argmax):
+    """sha256 of one tree's outputs as little-endian float32 and uint32 bytes."""
+    import hashlib
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(out_max, dtype="<f4").tobytes())
+    h.update(np.ascontiguousarray(out_argmax, dtype="<u4").tobytes())
+    return h.hexdigest()
+
+
+def inputs_digest(xs):
+    import hashlib
+    h = hashlib.sha256()
+    for x in xs:
+        h.update(np.ascontiguousarray(x, dtype="<f4").tobytes())
+    return h.hexdigest()

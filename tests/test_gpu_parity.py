@@ -15,31 +15,11 @@ import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-# (rank, nfreq, nt, subbands, primary trees as (num_early_triggers, max_width), beams_per_gpu, beams_per_batch)
-FP32_CASES = [
-    (6, 100, 128, [1], [(0, 4)], 1, 1),
-    (8, 640, 256, [2, 2, 1], [(0, 16), (1, 8)], 2, 1),
-    (9, 300, 256, [1, 1, 1], [(1, 32), (0, 8), (1, 2)], 2, 2),
-    (10, 1024, 512, [0, 0, 1], [(0, 32), (0, 16), (0, 8)], 1, 1),
-    (11, 2000, 256, [3, 5, 3, 1], [(2, 8), (1, 4)], 4, 2),
-    (7, 50, 128, [1, 1], [(0, 1), (0, 2)], 3, 1),
-    # explicit output time downsampling (third entry): 16 and 32 (saturated boxcar levels, partial
-    # 32-output tiles), 64, 2 and 1
-    (8, 256, 512, [0, 1, 1], [(0, 32, 16), (0, 16, 32)], 2, 1),
-    (7, 128, 512, [1, 1], [(0, 8, 64), (0, 4, 2), (0, 2, 1)], 1, 1),
-]
+FP32_CASES = H.PARITY_CASES
 
 
 def _cfg(case, dtype="float32"):
-    rank, nfreq, nt, sb, pts, bpg, bpb = case
-    prim = []
-    for ip, pt in enumerate(pts):
-        net, w = pt[:2]
-        tds = pt[2] if len(pt) > 2 else 0
-        prim.append(dict(num_early_triggers=net, max_width=w, dm_downsampling=0, time_downsampling=tds,
-                         wt_dm_downsampling=2 ** ((rank - (1 if ip else 0) - net) // 2), wt_time_downsampling=max(16, tds)))
-    return H.toy_config(rank=rank, nfreq=nfreq, nt=nt, dtype=dtype, subbands=sb, beams_per_gpu=bpg,
-                        beams_per_batch=bpb, num_active_batches=1, primary_trees=prim)
+    return H.case_config(case, dtype)
 
 
 @pytest.mark.parametrize("case", FP32_CASES, ids=lambda c: "r%d_f%d_t%d" % (c[0], c[1], c[2]))
