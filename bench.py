@@ -11,7 +11,12 @@ src_lib/GpuDedisperser.cpp:1598,1676). Prints one JSON line.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--beams B] [--dtype float16] [--impl reference]
 
 Multi-GPU: the path shards by beam with no exchange step, so N GPUs run N independent replicas
-(one process per GPU under torchrun); value = all ranks' beams over the max-over-ranks time.
+(one process per GPU under torchrun; run without torchrun, --gpus N > 1 launches torchrun itself);
+value = all ranks' beams over the max-over-ranks time.
+
+Also reported on one GPU: the plain fp32 path (one beam, float32 storage and input, no batching;
+BASELINE's config 2 shape) as 'plain_fp32', and the number of beams whose lag state fits in HBM as
+'capacity_beams'.
 """
 
 import argparse
@@ -257,24 +262,94 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     ems = replicas.max_over_ranks(f0.elapsed_time(f1))
 
+    # Beams whose state fits in this GPU's HBM at this plan: total memory over the device bytes per beam.
+    per_beam = dd.device_bytes() / float(args.beams)
+    capacity_beams = int(torch.cuda.get_device_properties(dev).total_memory // per_beam)
+
     alg = dd.algorithmic_bytes()
     # The gridding class reads int4 data and scales/offsets instead of storage-dtype samples.
     alg[0] += float(plan.beams_per_batch) * plan.nfreq * (plan.nt_in / 2 + plan.nt_in / 256 * 4 - plan.nt_in * esize)
     return dict(plan=plan, dd=dd, ms_per_step=ms_per_step, e2e_ms_per_step=ems / e2e_steps, ktimes=ktimes,
                 alg=alg, clocks=clk.summary(), h2d=h2d, d2h=d2h, device_bytes=dd.device_bytes(),
-                kernels_per_batch=dd.kernels_per_batch())
+                kernels_per_batch=dd.kernels_per_batch(), capacity_beams=capacity_beams,
+                bytes_per_beam=per_beam)
 
 
-def cpu_sample(nchunks=1, dtype="float16"):
-    """Times the CPU oracle (fp32 restatement of pirate's ReferenceDedisperser, sophistication 1)
-    on one beam of the bench workload; returns seconds per chunk."""
+def run_plain_fp32(args, steps):
+    """The plain fp32 GPU path (BASELINE config 2's shape): one beam, float32 storage, float32 N(0,1)
+    input resident in the input slot (no int4 input, no batching), same plan otherwise. Returns
+    (real-time beams, ms per step)."""
+    import torch
+    import pirate_b200 as pb
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    cfg = bench_config(1, "float32", args.rank, args.npri, args.nfreq)
+    plan = pb.DedispersionPlan(pb.DedispersionConfig.from_dict(cfg))
+    dd = pb.GpuDedisperser(plan, cuda_device_id=dev, num_consumers=1)
+    dd.allocate()
+    import numpy as np
+    for i, t in enumerate(plan.trees):
+        arr = np.ones((dd.nbatches_wt, 1, t.ndm_wt, t.nt_wt, t.nprofiles, t.nsubbands), np.float32)
+        dd.fill_all_weights(i, arr)
+    stream = torch.cuda.current_stream()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(99)
+    x = torch.randn((1, plan.nfreq, plan.nt_in), generator=g, device="cuda", dtype=torch.float32)
+    seq = [0]
+
+    def step():
+        s = seq[0]
+        a = dd.acquire_input(s, stream)
+        if s == 0:
+            a.copy_(x)
+        dd.release_input_and_launch_dd_kernels(s, stream)
+        dd.acquire_output(0, s, stream)
+        dd.release_output(0, s, stream)
+        seq[0] += 1
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    del dd
+    torch.cuda.empty_cache()
+    return CHUNK_SECONDS / (ms * 1e-3), ms
+
+
+def cpu_kind():
+    """'reference' when pirate's own reference CPU sources were compiled as oracle/_ref (travels with
+    the repository as a built file), else 'port' (the oracle's restatement)."""
+    return "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libpirate_ref.so")) else "port"
+
+
+def cpu_sample(nchunks=1, dtype="float16", kind=None):
+    """Times pirate's CPU ReferenceDedisperser (sophistication 1: two-stage trees with lagged
+    downsampling, pirate's GPU algorithm) on one beam of the bench workload, single-threaded: pirate's
+    own code from oracle/_ref when it is built, else the oracle's fp32 restatement of it. The int4 chunk
+    is dequantized first (ReferenceDequantizationKernel's arithmetic), as pirate's timing loop does.
+    Returns seconds per chunk."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle
+    kind = kind or cpu_kind()
     cfg = bench_config(1, "float32")
     cfg["dtype"] = dtype if dtype != "bfloat16" else "float16"   # same plan shapes as the GPU run
-    orc = oracle.OracleDedisperser(cfg, 1, 32)
-    ws = [oracle.bare_weights(orc.wt_shape(i), orc.trees[i]["nprofiles"]) for i in range(orc.ntrees)]
+    if kind == "reference":
+        import pirate_ref
+        ref = pirate_ref.PirateReferenceDedisperser(cfg, sophistication=1)
+        shapes = [(1, t["ndm_wt"], t["nt_wt"], t["nprofiles"], t["N"]) for t in ref.trees]
+        ws = [oracle.bare_weights(sh, t["nprofiles"]) for sh, t in zip(shapes, ref.trees)]
+        run = lambda x: ref.dedisperse(x, ws)   # noqa: E731
+    else:
+        orc = oracle.OracleDedisperser(cfg, 1, 32)
+        ws = [oracle.bare_weights(orc.wt_shape(i), orc.trees[i]["nprofiles"]) for i in range(orc.ntrees)]
+        run = lambda x: orc.dedisperse(0, x, ws)   # noqa: E731
     # The same int4 input format as the GPU run, dequantized (ReferenceDequantizationKernel) and then
     # dedispersed, as pirate's timing loop does per chunk.
     rng = np.random.default_rng(0)
@@ -287,7 +362,7 @@ def cpu_sample(nchunks=1, dtype="float16"):
     t0 = time.time()
     for _ in range(nchunks):
         x = oracle.dequantize(data, so, 1, 16384, CHUNK)
-        orc.dedisperse(0, x, ws)
+        run(x)
     return (time.time() - t0) / nchunks
 
 
@@ -296,8 +371,9 @@ def _cpu_worker(q, nchunks, dtype):
 
 
 def run_reference(args, rank, world):
-    """The reference arm: pirate's CPU dedisperser (restated by the oracle; pirate itself needs ksgpu,
-    yaml-cpp and MKL, which are not installed) on the host cores, one beam per process."""
+    """The reference arm: pirate's CPU ReferenceDedisperser on the host cores, one beam per process
+    (about 24 GB each at rank 16): pirate's own sources compiled as oracle/_ref, or, where that build is
+    absent, the oracle's restatement."""
     if rank != 0:
         return None
     import multiprocessing as mp
@@ -327,7 +403,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--beams", type=int, default=4)
+    ap.add_argument("--beams", type=int, default=8)
+    ap.add_argument("--no-plain-fp32", action="store_true")
     ap.add_argument("--dtype", default="float16", choices=["float16", "bfloat16", "float32"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -339,8 +416,19 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # One process per GPU: relaunch under torchrun (rendezvous on 127.0.0.1).
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if world != args.gpus:
+        sys.exit("bench.py: --gpus %d but WORLD_SIZE=%d" % (args.gpus, world))
     cfg_json = {"workload": "rank-16 tree, 16384 channels 400-800 MHz, 5 primary trees (time downsampling 1-16), "
                             "2048-sample chunks, widths to 32 per tree, full-band search",
                 "beams_per_gpu": args.beams, "chunk_samples": CHUNK, "sample_ms": SAMPLE_MS,
@@ -359,9 +447,11 @@ def main():
                     "steps": 1, "warmup": 0, "ms_per_step": r["sec"] * 1e3, "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1)",
                     "config": cfg_json,
-                    "cpu_baseline": {"value": r["value"], "unit": "beams", "cores": r["nproc"], "kind": "port",
-                                     "sample": "1 chunk of 1 beam per process, %d processes (fp32 oracle: int4 dequantization, then "
-                                               "ReferenceDedisperser sophistication 1)" % r["nproc"]},
+                    "cpu_baseline": {"value": r["value"], "unit": "beams", "cores": r["nproc"], "kind": cpu_kind(),
+                                     "sample": "1 chunk of 1 beam per process, %d processes (int4 dequantization, then pirate's "
+                                               "ReferenceDedisperser sophistication 1, %s)" % (
+                                                   r["nproc"], "pirate's own code, oracle/_ref" if cpu_kind() == "reference"
+                                                   else "the oracle's fp32 restatement")},
                     "e2e": {"value": r["value"], "unit": "beams", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
             print(json.dumps(line), flush=True)
         if world > 1:
@@ -382,7 +472,7 @@ def main():
     value = real_time_beams(args.beams, world, r["ms_per_step"] * 1e-3, CHUNK_SECONDS)
     e2e = real_time_beams(args.beams, world, r["e2e_ms_per_step"] * 1e-3, CHUNK_SECONDS)
 
-    classes = ["grid_lds", "unused", "stage1", "stage2", "pf"]
+    classes = ["grid_lds", "sifter", "stage1", "stage2", "pf"]
     kt = r["ktimes"]
     tot_ms = sum(kt[c][0] for c in classes)
     dom = max(classes, key=lambda c: kt[c][0])
@@ -428,11 +518,25 @@ def main():
                 "pipeline_alg_GBps": round(e2e_alg_gbs, 1),
                 "device_bytes": r["device_bytes"],
                 "clocks": r["clocks"]}
+        line["capacity_beams"] = r["capacity_beams"]
+        line["capacity_note"] = ("beams whose lag state and buffers fit in this GPU's HBM (%.2f GB per beam); "
+                                 "the real-time figure above is throughput" % (r["bytes_per_beam"] / 1e9))
+    if world == 1 and not args.no_plain_fp32:
+        del r["dd"]
+        import gc
+        gc.collect()
+        pv, pms = run_plain_fp32(args, max(10, min(args.steps, 30)))
+        line["plain_fp32"] = {"value": round(pv, 2), "unit": "beams", "ms_per_step": round(pms, 4),
+                              "config": "1 beam, float32 storage, float32 input resident on the device, no batching"}
+        line["vs_plain_fp32"] = round(value / pv, 3)
+    if rank == 0:
         if not args.no_cpu_baseline and world == 1:
-            sec = cpu_sample(1, args.dtype)
-            line["cpu_baseline"] = {"value": round(CHUNK_SECONDS / sec, 4), "unit": "beams", "cores": 1, "kind": "port",
-                                    "sample": "1 chunk of 1 beam (fp32 oracle: ReferenceDequantizationKernel then "
-                                              "ReferenceDedisperser sophistication 1), %.1f s" % sec}
+            kind = cpu_kind()
+            sec = cpu_sample(1, args.dtype, kind)
+            line["cpu_baseline"] = {"value": round(CHUNK_SECONDS / sec, 4), "unit": "beams", "cores": 1, "kind": kind,
+                                    "sample": "1 chunk of 1 beam, %.1f s: int4 dequantization, then pirate's ReferenceDedisperser "
+                                              "sophistication 1 (%s)" % (sec, "pirate's own code, oracle/_ref" if kind == "reference"
+                                                                        else "the oracle's fp32 restatement")}
         print(json.dumps(line), flush=True)
 
     if world > 1:

@@ -104,6 +104,11 @@ typedef struct pb2_dd_params {
     long num_consumers;
     int synchronous;
     long initial_chunk;
+    /* pb2_dd_release_input blocks until every consumer has released seq_id - nbatches_out (pirate's
+     * blocking wait on the release-output event ring, src_lib/GpuDedisperser.cpp:1078-1081), and
+     * pb2_dd_acquire_output blocks until seq_id has been launched (src_lib/GpuDedisperser.cpp:932);
+     * after this many milliseconds they fail instead (0 -> 60000). */
+    long release_timeout_ms;
 } pb2_dd_params;
 
 /* GpuDedisperser::Outputs, include/pirate/Dedisperser.hpp:98-125. out_max[i] and out_argmax[i] are
@@ -114,6 +119,16 @@ typedef struct pb2_outputs {
     long ndm_out[PB2_MAX_TREES], nt_out[PB2_MAX_TREES];
     void *out_max[PB2_MAX_TREES];
     uint32_t *out_argmax[PB2_MAX_TREES];
+    /* Candidate stage (pb2_dd_enable_sifter), else null. Device arrays of nbeams entries: each beam's
+     * strongest output over every tree (the toy grouper's reduction, pirate_frb/run_toy_grouper.py:79-116):
+     * cand_peak, cand_tree, cand_idm, cand_itime, cand_token; cand_valid = (peak >= threshold); the
+     * fp16 patch (nbeams, 1728) around the peak; and the score (the sifter's logit, or the peak when no
+     * sifter is attached; -inf where not valid). */
+    float *cand_peak;
+    int *cand_tree, *cand_idm, *cand_itime, *cand_valid;
+    uint32_t *cand_token;
+    uint16_t *patches;
+    float *scores;
 } pb2_outputs;
 
 /* The toy grouper's per-chunk reduction (pirate_frb/run_toy_grouper.py:79-116), as one kernel on
@@ -200,15 +215,44 @@ int pb2_dd_fill_analytic_weights(pb2_dedisperser *dd, const double *freq_varianc
 /* GpuDedisperser::stop, src_lib/GpuDedisperser.cpp:735 */
 int pb2_dd_stop(pb2_dedisperser *dd);
 /* Kernel launches per (chunk, batch), and algorithmic HBM bytes per (chunk, batch) for the
- * kernel classes [grid+lds (one fused kernel), unused, stage1, stage2, pf]. */
+ * kernel classes [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf]. */
 int pb2_dd_kernels_per_batch(const pb2_dedisperser *dd, long *n);
 int pb2_dd_algorithmic_bytes(const pb2_dedisperser *dd, double *out5);
 /* Per-kernel-class CUDA-event timing on the dedisperser's compute stream (the analogue of pirate's
  * KernelTimer / ResourceTracker reporting, src_lib/GpuDedisperser.cpp:1674-1681). kernel_times()
- * synchronizes and returns accumulated milliseconds and launch counts for [grid+lds (one fused kernel), unused, stage1, stage2, pf]. */
+ * synchronizes and returns accumulated milliseconds and launch counts for [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf]. */
 int pb2_dd_enable_timing(pb2_dedisperser *dd, int on);
 int pb2_dd_kernel_times(pb2_dedisperser *dd, double *ms5, long *counts5);
 void pb2_dd_destroy(pb2_dedisperser *dd);
+
+/* ---- Learned candidate sifter (no counterpart in pirate: the north star's learned stage behind the
+ * threshold peak finder, which stays the fallback and the judge of its recall) ----
+ *
+ * Patch: 9 fine DMs (the peak's +-4) x 32 output times x 6 trailing boxcar widths (1..32) of the
+ * dedispersed data around a candidate, each boxcar sum / sqrt(width), fp16, layout (dm, time, width).
+ * MLP: 1728 -> 256 -> 128 -> 1 with ReLU, bf16 weights (fp32 master copy), FP32 accumulation on the
+ * tensor cores; trained on the mean binary cross-entropy of its logit with Adam. Parameters are fp32 in
+ * the order W1 (256, 1728), b1, W2 (128, 256), b2, W3 (1, 128), b3 (weights (out, in) row-major). */
+typedef struct pb2_sifter pb2_sifter;
+int pb2_sifter_create(int cuda_device_id, long max_batch, uint64_t seed, pb2_sifter **out);
+void pb2_sifter_destroy(pb2_sifter *s);
+int pb2_sifter_nparams(long *n);
+int pb2_sifter_set_params(pb2_sifter *s, const float *host_params);
+int pb2_sifter_get_params(const pb2_sifter *s, float *host_params);
+/* logits[n] (device) of n device patches (n, 1728) fp16, n <= max_batch, on 'stream'. */
+int pb2_sifter_forward(pb2_sifter *s, const void *patches, long n, float *logits, void *stream);
+/* Gradients of the mean binary cross-entropy over a batch (device labels 0/1) into host grad[nparams];
+ * *loss = the batch loss. Synchronizes 'stream'. */
+int pb2_sifter_gradients(pb2_sifter *s, const void *patches, const float *labels, long n, float *grad, double *loss,
+                         void *stream);
+/* One Adam step (0.9, 0.999, 1e-8) with learning rate lr; *loss = the batch loss. Synchronizes. */
+int pb2_sifter_train_step(pb2_sifter *s, const void *patches, const float *labels, long n, float lr, double *loss,
+                          void *stream);
+/* Adds the candidate stage to every later batch of 'dd' (after pb2_dd_allocate): per-beam peak over the
+ * trees, patches of peaks >= threshold (sigma), and scores by 'sifter' (may be null: scores are then the
+ * peaks). The results appear in pb2_outputs. The sifter then runs on the dedisperser's compute stream
+ * and must neither be trained meanwhile nor destroyed before the dedisperser. */
+int pb2_dd_enable_sifter(pb2_dedisperser *dd, float threshold, pb2_sifter *sifter);
 
 /* ---- Allocation-free single-chunk dedispersion (no counterpart in pirate) ----
  *

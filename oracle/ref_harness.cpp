@@ -15,6 +15,8 @@
 //                          out_max / out_argmax (include/pirate/Dedisperser.hpp:455-473)
 //   ref_eval_tokens(...)   ReferencePeakFindingKernel::eval_tokens (src_lib/PeakFindingKernel.cu:460)
 //   ref_self_tests(...)    ReferenceTree::test_basics/test_subbands, ReferenceLagbuf::test_random
+//   ref_pulse_*(...)       SinglePulse (src_lib/simpulse.cpp), with MKL's c2r DFT supplied by
+//                          oracle/ksgpu_shim/mkl_dfti.h
 
 #include "pirate/DedispersionConfig.hpp"
 #include "pirate/DedispersionPlan.hpp"
@@ -22,6 +24,7 @@
 #include "pirate/PeakFindingKernel.hpp"
 #include "pirate/ReferenceLagbuf.hpp"
 #include "pirate/ReferenceTree.hpp"
+#include "pirate/simpulse.hpp"
 
 #include <cstdint>
 #include <cstring>
@@ -31,6 +34,7 @@
 #include <vector>
 
 using namespace pirate;
+using pirate::simpulse::SinglePulse;
 
 namespace {
 
@@ -197,6 +201,74 @@ int ref_self_tests(long niter)
             ReferenceTree::test_subbands();
             ReferenceLagbuf::test_random();
         }
+    });
+}
+
+// SinglePulse (include/pirate/simpulse.hpp:40-119). p[9] = dm, sm, intrinsic_width, spectral_index,
+// undispersed_arrival_time_sec, time_sample_ms, snr, subband_freq_lo_MHz, subband_freq_hi_MHz.
+struct RefPulse
+{
+    ksgpu::Array<double> edges, var;
+    std::unique_ptr<SinglePulse> sp;
+};
+
+__attribute__((visibility("default")))
+void *ref_pulse_create(const double *p, long internal_nt, const double *freq_edges, const double *freq_variances, long nfreq)
+{
+    RefPulse *h = new RefPulse;
+    int rc = guard([&] {
+        h->edges = ksgpu::Array<double>({nfreq + 1}, ksgpu::af_uhost);
+        h->var = ksgpu::Array<double>({nfreq}, ksgpu::af_uhost);
+        memcpy(h->edges.data, freq_edges, (nfreq + 1) * sizeof(double));
+        memcpy(h->var.data, freq_variances, nfreq * sizeof(double));
+        SinglePulse::Params sp;
+        sp.dm = p[0]; sp.sm = p[1]; sp.intrinsic_width = p[2]; sp.spectral_index = p[3];
+        sp.undispersed_arrival_time_sec = p[4]; sp.time_sample_ms = p[5]; sp.snr = p[6];
+        sp.subband_freq_lo_MHz = p[7]; sp.subband_freq_hi_MHz = p[8];
+        sp.internal_nt = internal_nt;
+        sp.freq_edges_MHz = h->edges;
+        sp.freq_variances = h->var;
+        h->sp.reset(new SinglePulse(sp));
+    });
+    if (rc != 0) { delete h; return nullptr; }
+    return h;
+}
+
+__attribute__((visibility("default"))) void ref_pulse_destroy(void *h) { delete (RefPulse *) h; }
+
+// out[3] = it_start, it_end, number of stored samples.
+__attribute__((visibility("default")))
+int ref_pulse_range(void *hv, long *out)
+{
+    return guard([&] {
+        const SinglePulse &sp = *((RefPulse *) hv)->sp;
+        out[0] = sp.it_start; out[1] = sp.it_end; out[2] = sp.sparse_data.size;
+    });
+}
+
+__attribute__((visibility("default")))
+int ref_pulse_sparse(void *hv, long *freq_it0, long *freq_nt, long *freq_sd_off, float *sparse_data)
+{
+    return guard([&] {
+        const SinglePulse &sp = *((RefPulse *) hv)->sp;
+        long nfreq = sp.freq_it0.size;
+        memcpy(freq_it0, sp.freq_it0.data, nfreq * sizeof(long));
+        memcpy(freq_nt, sp.freq_nt.data, nfreq * sizeof(long));
+        memcpy(freq_sd_off, sp.freq_sd_off.data, nfreq * sizeof(long));
+        memcpy(sparse_data, sp.sparse_data.data, sp.sparse_data.size * sizeof(float));
+    });
+}
+
+// SinglePulse::add_to_timestream on a C-contiguous (nfreq, nt) float32 array starting at out_it0.
+__attribute__((visibility("default")))
+int ref_pulse_add_to_timestream(void *hv, float *out, long nfreq, long nt, long out_it0, float weight)
+{
+    return guard([&] {
+        const SinglePulse &sp = *((RefPulse *) hv)->sp;
+        ksgpu::Array<float> a({nfreq, nt}, ksgpu::af_uhost);
+        memcpy(a.data, out, nfreq * nt * sizeof(float));
+        sp.add_to_timestream(a, out_it0, weight);
+        memcpy(out, a.data, nfreq * nt * sizeof(float));
     });
 }
 

@@ -37,14 +37,18 @@ class _TreeInfo(ctypes.Structure):
 
 class _DdParams(ctypes.Structure):
     _fields_ = [("cuda_device_id", ctypes.c_int), ("nbatches_out", ctypes.c_long), ("nbatches_wt", ctypes.c_long),
-                ("num_consumers", ctypes.c_long), ("synchronous", ctypes.c_int), ("initial_chunk", ctypes.c_long)]
+                ("num_consumers", ctypes.c_long), ("synchronous", ctypes.c_int), ("initial_chunk", ctypes.c_long),
+                ("release_timeout_ms", ctypes.c_long)]
 
 
 class _Outputs(ctypes.Structure):
     _fields_ = [("dtype", ctypes.c_int), ("nbeams", ctypes.c_long), ("ichunk_zero_based", ctypes.c_long),
                 ("ichunk_fpga_based", ctypes.c_long), ("ibeam", ctypes.c_long), ("ntrees", ctypes.c_long),
                 ("ndm_out", ctypes.c_long * MAX_TREES), ("nt_out", ctypes.c_long * MAX_TREES),
-                ("out_max", ctypes.c_void_p * MAX_TREES), ("out_argmax", ctypes.c_void_p * MAX_TREES)]
+                ("out_max", ctypes.c_void_p * MAX_TREES), ("out_argmax", ctypes.c_void_p * MAX_TREES),
+                ("cand_peak", ctypes.c_void_p), ("cand_tree", ctypes.c_void_p), ("cand_idm", ctypes.c_void_p),
+                ("cand_itime", ctypes.c_void_p), ("cand_valid", ctypes.c_void_p), ("cand_token", ctypes.c_void_p),
+                ("patches", ctypes.c_void_p), ("scores", ctypes.c_void_p)]
 
 
 def lib():
@@ -99,6 +103,15 @@ def lib():
         "pb2_dd_enable_timing": (ctypes.c_int, [vp, ctypes.c_int]),
         "pb2_dd_kernel_times": (ctypes.c_int, [vp, dp, lp]),
         "pb2_dd_destroy": (None, [vp]),
+        "pb2_sifter_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_long, ctypes.c_uint64, ctypes.POINTER(vp)]),
+        "pb2_sifter_destroy": (None, [vp]),
+        "pb2_sifter_nparams": (ctypes.c_int, [lp]),
+        "pb2_sifter_set_params": (ctypes.c_int, [vp, vp]),
+        "pb2_sifter_get_params": (ctypes.c_int, [vp, vp]),
+        "pb2_sifter_forward": (ctypes.c_int, [vp, vp, ctypes.c_long, vp, vp]),
+        "pb2_sifter_gradients": (ctypes.c_int, [vp, vp, vp, ctypes.c_long, vp, dp, vp]),
+        "pb2_sifter_train_step": (ctypes.c_int, [vp, vp, vp, ctypes.c_long, ctypes.c_float, dp, vp]),
+        "pb2_dd_enable_sifter": (ctypes.c_int, [vp, ctypes.c_float, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -366,6 +379,19 @@ class Outputs:
         # uint32 tokens, exposed as int32 views (same bits).
         self.out_argmax = [_device_tensor(o.out_argmax[i], (o.nbeams, o.ndm_out[i], o.nt_out[i]), "int32", device)
                            for i in range(o.ntrees)]
+        # Candidate stage (GpuDedisperser.enable_sifter), else None: per-beam device tensors.
+        self.candidates = None
+        if o.cand_peak:
+            B = o.nbeams
+            self.candidates = dict(
+                peak=_device_tensor(o.cand_peak, (B,), "float32", device),
+                tree=_device_tensor(o.cand_tree, (B,), "int32", device),
+                idm=_device_tensor(o.cand_idm, (B,), "int32", device),
+                itime=_device_tensor(o.cand_itime, (B,), "int32", device),
+                token=_device_tensor(o.cand_token, (B,), "int32", device),
+                valid=_device_tensor(o.cand_valid, (B,), "int32", device),
+                patches=_device_tensor(o.patches, (B, 9, 32, 6), "float16", device),
+                scores=_device_tensor(o.scores, (B,), "float32", device))
 
 
 class GpuDedisperser:
@@ -373,12 +399,12 @@ class GpuDedisperser:
     pirate_frb/GpuDedisperser.py:123-197)."""
 
     def __init__(self, plan, cuda_device_id=0, num_consumers=1, nbatches_out=0, nbatches_wt=0,
-                 initial_chunk=0, synchronous=True):
+                 initial_chunk=0, synchronous=True, release_timeout_ms=0):
         self.plan = plan
         self.cuda_device_id = int(cuda_device_id)
         self.device = "cuda:%d" % self.cuda_device_id
         p = _DdParams(self.cuda_device_id, int(nbatches_out), int(nbatches_wt), int(num_consumers),
-                      1 if synchronous else 0, int(initial_chunk))
+                      1 if synchronous else 0, int(initial_chunk), int(release_timeout_ms))
         h = ctypes.c_void_p()
         _check(lib().pb2_dd_create(plan._h, ctypes.byref(p), ctypes.byref(h)))
         self._h = h
@@ -404,12 +430,12 @@ class GpuDedisperser:
         return n.value
 
     def algorithmic_bytes(self):
-        """HBM bytes per (chunk, batch) for [grid_lds, unused, stage1, stage2, pf]."""
+        """HBM bytes per (chunk, batch) for [grid_lds, sifter (0), stage1, stage2, pf]."""
         out = (ctypes.c_double * 5)()
         _check(lib().pb2_dd_algorithmic_bytes(self._h, out))
         return list(out)
 
-    KERNEL_CLASSES = ("grid_lds", "unused", "stage1", "stage2", "pf")
+    KERNEL_CLASSES = ("grid_lds", "sifter", "stage1", "stage2", "pf")
 
     def enable_timing(self, on=True):
         _check(lib().pb2_dd_enable_timing(self._h, 1 if on else 0))
@@ -470,6 +496,14 @@ class GpuDedisperser:
 
     def stop(self):
         _check(lib().pb2_dd_stop(self._h))
+
+    def enable_sifter(self, threshold=6.0, sifter=None):
+        """Adds the candidate stage to every later batch: each beam's strongest output over the trees,
+        the fp16 patch (9 DM x 32 time x 6 width) of peaks >= threshold, and its score by 'sifter'
+        (pirate_b200.sifter.Sifter, or None: the score is then the peak). Results appear in
+        Outputs.candidates. The sifter must not be trained while attached."""
+        self._sifter = sifter
+        _check(lib().pb2_dd_enable_sifter(self._h, float(threshold), sifter._h if sifter is not None else None))
 
     @contextlib.contextmanager
     def get_input(self, stream=None):

@@ -6,6 +6,7 @@
 #include "avar.hpp"
 #include "kernels.cuh"
 #include "simpulse.hpp"
+#include "sifter.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -18,6 +19,7 @@ using namespace pb2;
 struct pb2_config { DedispersionConfig c; };
 struct pb2_plan { std::shared_ptr<DedispersionPlan> p; };
 struct pb2_dedisperser { std::unique_ptr<GpuDedisperser> d; };
+struct pb2_sifter { std::unique_ptr<Sifter> s; };
 
 #define CUDA_CHECK(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) \
     throw std::runtime_error(std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
@@ -379,6 +381,7 @@ int pb2_dd_create(const pb2_plan *plan, const pb2_dd_params *p, pb2_dedisperser 
         gp.num_consumers = p->num_consumers;
         gp.synchronous = p->synchronous != 0;
         gp.initial_chunk = p->initial_chunk;
+        gp.release_timeout_ms = p->release_timeout_ms;
         *out = new pb2_dedisperser{std::unique_ptr<GpuDedisperser>(new GpuDedisperser(*plan->p, gp))};
     });
 }
@@ -453,6 +456,14 @@ int pb2_dd_acquire_output(pb2_dedisperser *dd, long consumer_id, long seq_id, vo
             out->out_max[i] = o.out_max[i];
             out->out_argmax[i] = o.out_argmax[i];
         }
+        out->cand_peak = o.cand_peak;
+        out->cand_tree = o.cand_tree;
+        out->cand_idm = o.cand_idm;
+        out->cand_itime = o.cand_itime;
+        out->cand_valid = o.cand_valid;
+        out->cand_token = o.cand_token;
+        out->patches = o.patches;
+        out->scores = o.scores;
     });
 }
 
@@ -501,6 +512,60 @@ int pb2_dd_kernel_times(pb2_dedisperser *dd, double *ms5, long *counts5)
 }
 
 void pb2_dd_destroy(pb2_dedisperser *dd) { delete dd; }
+
+int pb2_sifter_create(int cuda_device_id, long max_batch, uint64_t seed, pb2_sifter **out)
+{
+    return guard([&] { REQUIRE_PTR(out); *out = new pb2_sifter{std::unique_ptr<Sifter>(new Sifter(cuda_device_id, max_batch, seed))}; });
+}
+
+void pb2_sifter_destroy(pb2_sifter *s) { delete s; }
+
+int pb2_sifter_nparams(long *n)
+{
+    return guard([&] { REQUIRE_PTR(n); *n = Sifter::nparams(); });
+}
+
+int pb2_sifter_set_params(pb2_sifter *s, const float *host_params)
+{
+    return guard([&] { REQUIRE_PTR(s); REQUIRE_PTR(host_params); s->s->set_params(host_params); });
+}
+
+int pb2_sifter_get_params(const pb2_sifter *s, float *host_params)
+{
+    return guard([&] { REQUIRE_PTR(s); REQUIRE_PTR(host_params); s->s->get_params(host_params); });
+}
+
+int pb2_sifter_forward(pb2_sifter *s, const void *patches, long n, float *logits, void *stream)
+{
+    return guard([&] {
+        REQUIRE_PTR(s); REQUIRE_PTR(patches); REQUIRE_PTR(logits);
+        CUDA_CHECK(cudaSetDevice(s->s->device));
+        s->s->forward((const uint16_t *) patches, n, logits, (cudaStream_t) stream);
+    });
+}
+
+int pb2_sifter_gradients(pb2_sifter *s, const void *patches, const float *labels, long n, float *grad, double *loss,
+                         void *stream)
+{
+    return guard([&] {
+        REQUIRE_PTR(s); REQUIRE_PTR(patches); REQUIRE_PTR(labels); REQUIRE_PTR(grad); REQUIRE_PTR(loss);
+        *loss = s->s->gradients((const uint16_t *) patches, labels, n, grad, (cudaStream_t) stream);
+    });
+}
+
+int pb2_sifter_train_step(pb2_sifter *s, const void *patches, const float *labels, long n, float lr, double *loss,
+                          void *stream)
+{
+    return guard([&] {
+        REQUIRE_PTR(s); REQUIRE_PTR(patches); REQUIRE_PTR(labels); REQUIRE_PTR(loss);
+        *loss = s->s->train_step((const uint16_t *) patches, labels, n, lr, (cudaStream_t) stream);
+    });
+}
+
+int pb2_dd_enable_sifter(pb2_dedisperser *dd, float threshold, pb2_sifter *sifter)
+{
+    return guard([&] { REQUIRE_PTR(dd); dd->d->enable_sifter(threshold, sifter ? sifter->s.get() : nullptr); });
+}
 
 int pb2_dedisperse_chunk_noalloc(const pb2_plan *plan, const void *in, const float *const *weights,
                                  void *const *out_max, uint32_t *const *out_argmax, void *stream)

@@ -4,6 +4,7 @@
 #include "avar.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <sstream>
 #include <stdexcept>
@@ -86,7 +87,12 @@ void GpuDedisperser::check_alive() const
 template<typename F>
 auto GpuDedisperser::entry(F &&f) -> decltype(f())
 {
-    std::lock_guard<std::mutex> lk(mtx);
+    std::unique_lock<std::mutex> lk(mtx);
+    struct Scope {
+        std::unique_lock<std::mutex> *&slot;
+        Scope(std::unique_lock<std::mutex> *&s, std::unique_lock<std::mutex> *l) : slot(s) { slot = l; }
+        ~Scope() { slot = nullptr; }
+    } scope(cur_lock, &lk);
     check_alive();
     try {
         return f();
@@ -102,11 +108,67 @@ void GpuDedisperser::stop(std::exception_ptr e)
     std::lock_guard<std::mutex> lk(mtx);
     if (!error && e) error = e;
     stopped = true;
+    cv.notify_all();
 }
 
 int GpuDedisperser::kernels_per_batch() const
 {
-    return 1 + int(plan.num_primary_trees) + stage2_launches() + int(plan.ntrees);
+    // candidate stage: beam peaks, patches, then the MLP (3 GEMMs) and the score mask, or the mask alone
+    const int cand = sift ? (2 + (sifter ? 4 : 1)) : 0;
+    return 1 + int(plan.num_primary_trees) + stage2_launches() + int(plan.ntrees) + cand;
+}
+
+void GpuDedisperser::enable_sifter(float threshold, Sifter *sf)
+{
+    entry([&]() {
+        if (!allocated) throw runtime_error("GpuDedisperser::enable_sifter(): allocate() was not called");
+        if (plan.ntrees > kPatchMaxTrees) throw runtime_error("GpuDedisperser::enable_sifter(): too many trees");
+        if (sf && (sf->device != params.cuda_device_id || sf->max_batch < B))
+            throw runtime_error("GpuDedisperser::enable_sifter(): the sifter must be on this device with max_batch >= beams_per_batch");
+        CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
+        CUDA_CHECK(cudaStreamSynchronize(compute));
+        if (!d_cand.ptr) {
+            d_cand.alloc(size_t(nbatches_out) * 8 * B * 4);
+            d_patches.alloc(size_t(nbatches_out) * B * kPatchLen * sizeof(uint16_t));
+        }
+        memset(&patch_args, 0, sizeof(patch_args));
+        patch_args.ntrees = int(plan.ntrees);
+        for (long i = 0; i < plan.ntrees; i++) {
+            const DedispersionTree &t = plan.trees[i];
+            const FrequencySubbands &fs = t.frequency_subbands;
+            PatchTree &pt = patch_args.t[i];
+            if (fs.pf_rank > 4) throw runtime_error("GpuDedisperser::enable_sifter(): peak-finding rank above 4");
+            if (s2[i].pf_cap < 64) throw runtime_error("GpuDedisperser::enable_sifter(): subband rows hold fewer than 64 samples");
+            pt.pf = s2[i].pfring.ptr;
+            pt.pf_cap = s2[i].pf_cap;
+            pt.M = int(fs.M);
+            pt.ndm_out = int(t.ndm_out);
+            pt.nt_ds = int(t.nt_ds);
+            pt.Dout = int(t.pf.time_downsampling);
+            pt.Dcore = int(t.Dcore);
+            pt.pf_rank = int(fs.pf_rank);
+            for (int d = 0; d < 16; d++) pt.d_to_m[d] = -1;
+            pt.nfull = -1;
+            for (long m = 0; m < fs.M; m++) {
+                long n = fs.m_to_n[m];
+                if (fs.n_to_flo[n] == 0 && fs.n_to_fhi[n] == pow2(fs.pf_rank)) {
+                    pt.d_to_m[fs.m_to_d[m]] = int(m);
+                    pt.nfull = int(n);
+                }
+            }
+            if (pt.nfull < 0) throw runtime_error("GpuDedisperser::enable_sifter(): a tree without a full-band search");
+            pt.ndm_wt = int(t.ndm_wt);
+            pt.nt_wt = int(t.nt_wt);
+            pt.nt_out = int(t.nt_out);
+            pt.P = int(t.nprofiles);
+            pt.N = int(fs.N);
+        }
+        patch_args.threshold = threshold;
+        patch_args.B = int(B);
+        sift = true;
+        sift_threshold = threshold;
+        sifter = sf;
+    });
 }
 
 // Stage-2 launches per batch: runs of consecutive output trees with the same stage-2 kernel (same dd
@@ -372,12 +434,35 @@ void GpuDedisperser::release_input_and_launch_dd_kernels(long seq_id, cudaStream
     entry([&]() {
         if (seq_id != next_rel_in || seq_id >= next_acq_in)
             throw runtime_error("GpuDedisperser::release_input_and_launch_dd_kernels(): expected seq_id=" + std::to_string(next_rel_in) + ", got " + std::to_string(seq_id));
+        // Output back-pressure: the batch writes output slot seq_id % nbatches_out, which every consumer
+        // must have released (as seq_id - nbatches_out) first. Like pirate's blocking wait on its
+        // release-output event ring, wait for that release on the host (other threads release while
+        // this one waits), with a bound.
+        if (seq_id >= nbatches_out && params.num_consumers > 0) {
+            const long need = seq_id - nbatches_out;
+            auto released = [&] {
+                if (stopped) return true;
+                for (long c = 0; c < params.num_consumers; c++)
+                    if (next_rel_out[c] <= need) return false;
+                return true;
+            };
+            const long tmo = params.release_timeout_ms > 0 ? params.release_timeout_ms : 60000;
+            if (!cv.wait_for(*cur_lock, std::chrono::milliseconds(tmo), released)) {
+                long c = 0;
+                while (next_rel_out[c] > need) c++;
+                throw runtime_error("GpuDedisperser::release_input_and_launch_dd_kernels(): consumer " + std::to_string(c) +
+                                    " has not released seq_id=" + std::to_string(need) + " within " + std::to_string(tmo) +
+                                    " ms (output slots are reused every nbatches_out=" + std::to_string(nbatches_out) + " batches)");
+            }
+            if (stopped) throw runtime_error("GpuDedisperser: stopped while waiting for an output release");
+        }
         long slot = seq_id % nslots_in;
         CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
         CUDA_CHECK(cudaEventRecord(ev_in_acquired[slot], stream));
         CUDA_CHECK(cudaStreamWaitEvent(compute, ev_in_acquired[slot], 0));
         launch_batch(seq_id);
         next_rel_in++;
+        cv.notify_all();
     });
 }
 
@@ -518,6 +603,47 @@ void GpuDedisperser::launch_batch(long seq_id)
         launch_pf(a, dtype_code, int(B), s);
         tick(4, t4);
     }
+    if (sift) {
+        // Candidate stage: per-beam peak over the trees, patches of the peaks >= threshold, scores.
+        cudaEvent_t t1 = tick(1, nullptr);
+        float *cb = (float *) d_cand.ptr + size_t(slot_out) * 8 * B;
+        BeamPeakArgs ba;
+        memset(&ba, 0, sizeof(ba));
+        ba.ntrees = int(plan.ntrees);
+        for (long i = 0; i < plan.ntrees; i++) {
+            const DedispersionTree &t = plan.trees[i];
+            size_t osz = size_t(B) * t.ndm_out * t.nt_out;
+            ba.ndm[i] = t.ndm_out;
+            ba.nt[i] = t.nt_out;
+            ba.out_max[i] = s2[i].out_max.as<char>() + size_t(slot_out) * osz * esize;
+            ba.out_argmax[i] = s2[i].out_argmax.as<uint32_t>() + size_t(slot_out) * osz;
+        }
+        ba.peak = cb;
+        ba.tree = (int *) (cb + B);
+        ba.idm = (int *) (cb + 2 * B);
+        ba.itime = (int *) (cb + 3 * B);
+        ba.token = (uint32_t *) (cb + 4 * B);
+        launch_beam_peaks(ba, dtype_code, B, s);
+        PatchArgs pa = patch_args;
+        for (long i = 0; i < plan.ntrees; i++) {
+            const DedispersionTree &t = plan.trees[i];
+            pa.t[i].wt = s2[i].wt.as<float>() + size_t(slot_wt) * size_t(B) * t.ndm_wt * t.nt_wt * t.nprofiles * s2[i].N;
+        }
+        pa.peak = ba.peak; pa.tree = ba.tree; pa.idm = ba.idm; pa.itime = ba.itime; pa.token = ba.token;
+        pa.valid = (int *) (cb + 5 * B);
+        pa.ichunk = ichunk;
+        pa.beam0 = beam0;
+        pa.patches = d_patches.as<uint16_t>() + size_t(slot_out) * B * kPatchLen;
+        launch_patches(pa, dtype_code, s);
+        float *logits = cb + 6 * B, *scores = cb + 7 * B;
+        if (sifter) {
+            sifter->forward(pa.patches, B, logits, s);
+            launch_mask_scores(logits, pa.valid, scores, int(B), s);
+        } else {
+            launch_mask_scores(ba.peak, pa.valid, scores, int(B), s);
+        }
+        tick(1, t1);
+    }
     CUDA_CHECK(cudaEventRecord(ev_out_done[slot_out], s));
     out_done_recorded[slot_out] = true;
 }
@@ -528,7 +654,15 @@ GpuDedisperser::Outputs GpuDedisperser::acquire_output(long consumer_id, long se
         if (consumer_id < 0 || consumer_id >= params.num_consumers) throw runtime_error("GpuDedisperser::acquire_output(): bad consumer_id");
         if (seq_id != next_acq_out[consumer_id])
             throw runtime_error("GpuDedisperser::acquire_output(): expected seq_id=" + std::to_string(next_acq_out[consumer_id]) + ", got " + std::to_string(seq_id));
-        if (seq_id >= next_rel_in) throw runtime_error("GpuDedisperser::acquire_output(): seq_id has not been launched");
+        if (seq_id >= next_rel_in) {
+            // As pirate's blocking wait on its cdd2 event ring (src_lib/GpuDedisperser.cpp:932): wait on
+            // the host, bounded, until another thread has launched seq_id.
+            const long tmo = params.release_timeout_ms > 0 ? params.release_timeout_ms : 60000;
+            if (!cv.wait_for(*cur_lock, std::chrono::milliseconds(tmo), [&] { return stopped || seq_id < next_rel_in; }))
+                throw runtime_error("GpuDedisperser::acquire_output(): seq_id=" + std::to_string(seq_id) +
+                                    " has not been launched within " + std::to_string(tmo) + " ms");
+            if (stopped) throw runtime_error("GpuDedisperser: stopped while waiting for a launch");
+        }
         if (params.synchronous && next_rel_out[consumer_id] != seq_id)
             throw runtime_error("GpuDedisperser::acquire_output(): synchronous consumer must release before acquiring the next batch");
         if (seq_id - next_rel_out[consumer_id] >= nbatches_out)
@@ -550,6 +684,17 @@ GpuDedisperser::Outputs GpuDedisperser::acquire_output(long consumer_id, long se
             o.out_max.push_back(s2[i].out_max.as<char>() + size_t(slot) * osz * esize);
             o.out_argmax.push_back(s2[i].out_argmax.as<uint32_t>() + size_t(slot) * osz);
         }
+        if (sift) {
+            float *cb = (float *) d_cand.ptr + size_t(slot) * 8 * B;
+            o.cand_peak = cb;
+            o.cand_tree = (int *) (cb + B);
+            o.cand_idm = (int *) (cb + 2 * B);
+            o.cand_itime = (int *) (cb + 3 * B);
+            o.cand_token = (uint32_t *) (cb + 4 * B);
+            o.cand_valid = (int *) (cb + 5 * B);
+            o.scores = cb + 7 * B;
+            o.patches = d_patches.as<uint16_t>() + size_t(slot) * B * kPatchLen;
+        }
         next_acq_out[consumer_id]++;
         return o;
     });
@@ -565,6 +710,7 @@ void GpuDedisperser::release_output(long consumer_id, long seq_id, cudaStream_t 
         CUDA_CHECK(cudaEventRecord(ev_out_released[consumer_id][slot], stream));
         out_released_recorded[consumer_id][slot] = true;
         next_rel_out[consumer_id]++;
+        cv.notify_all();
     });
 }
 

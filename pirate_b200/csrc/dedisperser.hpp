@@ -20,7 +20,9 @@
 
 #include "kernels.cuh"
 #include "plan.hpp"
+#include "sifter.hpp"
 
+#include <condition_variable>
 #include <exception>
 #include <memory>
 #include <mutex>
@@ -53,6 +55,11 @@ public:
         long num_consumers = 1;
         bool synchronous = true;
         long initial_chunk = 0;
+        // release_input_and_launch_dd_kernels(seq_id) waits (host side) until every consumer has
+        // released seq_id - nbatches_out, and acquire_output(seq_id) until seq_id has been launched,
+        // as pirate's blocking event-ring waits do (src_lib/GpuDedisperser.cpp:932, 1078-1081); they
+        // fail after this many ms (0 -> 60000).
+        long release_timeout_ms = 0;
     };
 
     struct Outputs
@@ -62,6 +69,15 @@ public:
         std::vector<long> ndm_out, nt_out;
         std::vector<void *> out_max;
         std::vector<uint32_t *> out_argmax;
+        // Candidate stage (enable_sifter), device arrays of nbeams entries, else null: each beam's
+        // strongest output over every tree (peak, tree, idm, itime, token), valid = peak >= threshold,
+        // its fp16 patch (nbeams, 1728) and score (sifter logit, or the peak without a sifter; -inf if
+        // not valid).
+        float *cand_peak = nullptr;
+        int *cand_tree = nullptr, *cand_idm = nullptr, *cand_itime = nullptr, *cand_valid = nullptr;
+        uint32_t *cand_token = nullptr;
+        uint16_t *patches = nullptr;
+        float *scores = nullptr;
     };
 
     GpuDedisperser(const DedispersionPlan &plan, const Params &params);
@@ -83,6 +99,12 @@ public:
     // per-channel input variances (nfreq values > 0), and waits until they are on the GPU.
     void fill_analytic_weights(const double *freq_variances, long nfreq);
     void stop(std::exception_ptr e = nullptr);
+    // Adds the candidate stage to every later batch, on the compute stream after peak finding: the
+    // per-beam peak over the trees, the candidate patch of peaks >= threshold, and (if 'sifter' is not
+    // null) its MLP score. Requires allocate(). The sifter is used on the compute stream from then on
+    // and must not be trained at the same time; it must outlive the dedisperser or a later
+    // enable_sifter() call.
+    void enable_sifter(float threshold, Sifter *sifter);
 
     // Device bytes held by allocate() (for reporting).
     size_t device_bytes() const { return total_bytes; }
@@ -91,11 +113,11 @@ public:
     int stage2_launches() const;
     // Bytes of HBM traffic per (chunk, batch) of each kernel class (algorithmic: each element read or
     // written once, following pirate's ResourceTracker model):
-    // [grid+lds (one fused kernel), unused, stage1, stage2, pf].
+    // [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf].
     std::vector<double> algorithmic_bytes() const;
 
     // Kernel timing: when enabled, CUDA events bracket each kernel class
-    // [grid+lds (one fused kernel), unused, stage1, stage2, pf] on the compute stream; kernel_times() synchronizes and returns
+    // [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf] on the compute stream; kernel_times() synchronizes and returns
     // the accumulated milliseconds and launch counts since the last reset.
     void enable_timing(bool on);
     void kernel_times(double *ms5, long *counts5);
@@ -110,6 +132,8 @@ private:
     void launch_batch(long seq_id);
 
     std::mutex mtx;
+    std::condition_variable cv;                     // signalled by release_output() and stop()
+    std::unique_lock<std::mutex> *cur_lock = nullptr;   // the lock held by the running entry point
     std::exception_ptr error;
     bool stopped = false;
     bool allocated = false;
@@ -157,6 +181,13 @@ private:
     std::vector<Stage2> s2;
     DeviceBuffer d_inputs, d_tree0, d_lds_state;
     DeviceBuffer d_qdata, d_qscoff;   // int4 input slots (allocated when nt is a multiple of 256)
+    // Candidate stage: per output slot, 8 arrays of B 4-byte entries (peak, tree, idm, itime, token,
+    // valid, logits, scores) and B patches.
+    bool sift = false;
+    float sift_threshold = 0.0f;
+    Sifter *sifter = nullptr;
+    DeviceBuffer d_cand, d_patches;
+    PatchArgs patch_args;
     void *acquire_slot(long seq_id, cudaStream_t stream, void **int4);
 };
 

@@ -7,7 +7,9 @@
 For every case it records:
   - the sha256 of the case's inputs (so a change of the input generator is detected),
   - per (seq_id, tree) the sha256 of pirate's out_max (float32) and out_argmax (uint32) bytes,
-  - the full outputs of cases whose outputs are small, for diagnostics.
+  - the full outputs of cases whose outputs are small, for diagnostics;
+  - for the pulses of tests/helpers.pulse_fixture_cases(), pirate's SinglePulse sparse representation
+    (src_lib/simpulse.cpp; MKL's complex-to-real DFT supplied by oracle/ksgpu_shim/mkl_dfti.h).
 It runs sophistication 1 (two-stage trees with lagged downsampling, pirate's GPU algorithm) and checks
 that sophistication 0 (one-stage trees on plainly downsampled input) and 2 (MegaRingbuf ring buffers)
 give the same bytes on the smaller cases. Every tree's Dcore is min(time_downsampling, 8), the rule of
@@ -71,6 +73,13 @@ def main():
                     arrays["%s/%d/%d/arg" % (case["name"], s, i)] = a[i]
         print("%-20s %3d seqs, %d trees, %.1f s, sophistication 0/2 checked: %s" %
               (case["name"], len(digests), len(ref.trees), time.time() - t0, soph_checked), flush=True)
+    # SinglePulse construction (src_lib/simpulse.cpp), MKL's c2r DFT supplied by oracle/ksgpu_shim/mkl_dfti.h.
+    for pc in H.pulse_fixture_cases():
+        sp = PR.PiratePulse(freq_edges_MHz=pc["edges"], freq_variances=pc["var"], **pc["params"])
+        meta[pc["name"]] = dict(kind="pulse", it_start=int(sp.it_start), it_end=int(sp.it_end))
+        for k in ("freq_it0", "freq_nt", "freq_sd_off", "sparse_data"):
+            arrays["%s/%s" % (pc["name"], k)] = getattr(sp, k)
+        print("%-20s %d samples in [%d, %d)" % (pc["name"], sp.sparse_data.size, sp.it_start, sp.it_end), flush=True)
     arrays["meta_json"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
     np.savez_compressed(OUT, **arrays)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")

@@ -211,3 +211,33 @@ def inputs_digest(xs):
     for x in xs:
         h.update(np.ascontiguousarray(x, dtype="<f4").tobytes())
     return h.hexdigest()
+
+
+def pulse_fixture_cases():
+    """SinglePulse cases whose construction by pirate's simpulse.cpp is committed as fixtures: channel
+    edges (regular and irregular), per-channel variances and the pulse parameters (dispersion,
+    scattering, intrinsic width, spectral index, arrival before and after zero, subband restriction)."""
+    out = []
+    pars = [
+        dict(dm=50.0, sm=0.0, intrinsic_width=1e-3, spectral_index=0.0, undispersed_arrival_time_sec=0.2,
+             time_sample_ms=1.0, snr=20.0),
+        dict(dm=300.0, sm=2.0, intrinsic_width=3e-4, spectral_index=-1.5, undispersed_arrival_time_sec=-0.5,
+             time_sample_ms=0.983, snr=12.0),
+        dict(dm=0.0, sm=0.5, intrinsic_width=0.0, spectral_index=2.0, undispersed_arrival_time_sec=1.0,
+             time_sample_ms=2.0, snr=50.0),
+        dict(dm=1200.0, sm=0.1, intrinsic_width=5e-3, spectral_index=0.7, undispersed_arrival_time_sec=0.0,
+             time_sample_ms=1.0, snr=8.0, subband_freq_lo_MHz=520.0, subband_freq_hi_MHz=610.0),
+        dict(dm=700.0, sm=4.0, intrinsic_width=2e-3, spectral_index=-0.5, undispersed_arrival_time_sec=0.37,
+             time_sample_ms=1.0, snr=30.0, internal_nt=512),
+    ]
+    for k, p in enumerate(pars):
+        rng = np.random.default_rng(500 + k)
+        nfreq = 256 if k == 4 else 64
+        if k % 2 == 0:
+            edges = np.linspace(400.0, 800.0, nfreq + 1)
+        else:
+            df = rng.uniform(0.2, 1.8, nfreq)
+            edges = 400.0 + 400.0 * np.concatenate([[0.0], np.cumsum(df)]) / df.sum()
+        var = rng.uniform(0.5, 2.0, nfreq)
+        out.append(dict(name="pulse%d" % k, params=p, edges=edges, var=var))
+    return out

@@ -138,3 +138,50 @@ class PirateReferenceDedisperser:
                                  out.ctypes.data) != 0:
             raise RuntimeError("pirate reference eval_tokens: " + _err())
         return out
+
+
+class PiratePulse:
+    """pirate's simpulse.SinglePulse (src_lib/simpulse.cpp), with MKL's complex-to-real DFT supplied by
+    oracle/ksgpu_shim/mkl_dfti.h. Exposes it_start, it_end, freq_it0, freq_nt, freq_sd_off, sparse_data."""
+
+    def __init__(self, dm, sm, intrinsic_width, spectral_index, undispersed_arrival_time_sec, time_sample_ms, snr,
+                 freq_edges_MHz, freq_variances, subband_freq_lo_MHz=0.0, subband_freq_hi_MHz=1.0e9, internal_nt=1024):
+        L = lib()
+        if not getattr(L, "_pulse_sigs", False):
+            L.ref_pulse_create.restype = vp
+            L.ref_pulse_create.argtypes = [c_double_p, ctypes.c_long, vp, vp, ctypes.c_long]
+            L.ref_pulse_destroy.argtypes = [vp]
+            L.ref_pulse_range.argtypes = [vp, c_long_p]
+            L.ref_pulse_sparse.argtypes = [vp, vp, vp, vp, vp]
+            L.ref_pulse_add_to_timestream.argtypes = [vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_float]
+            L._pulse_sigs = True
+        edges = np.ascontiguousarray(freq_edges_MHz, dtype=np.float64)
+        var = np.ascontiguousarray(freq_variances, dtype=np.float64)
+        p = (ctypes.c_double * 9)(dm, sm, intrinsic_width, spectral_index, undispersed_arrival_time_sec,
+                                  time_sample_ms, snr, subband_freq_lo_MHz, subband_freq_hi_MHz)
+        h = L.ref_pulse_create(p, int(internal_nt), edges.ctypes.data, var.ctypes.data, var.size)
+        if not h:
+            raise RuntimeError("pirate SinglePulse: " + _err())
+        self.h = h
+        self.nfreq = var.size
+        r = (ctypes.c_long * 3)()
+        L.ref_pulse_range(h, r)
+        self.it_start, self.it_end = r[0], r[1]
+        self.freq_it0 = np.zeros(self.nfreq, np.int64)
+        self.freq_nt = np.zeros(self.nfreq, np.int64)
+        self.freq_sd_off = np.zeros(self.nfreq, np.int64)
+        self.sparse_data = np.zeros(r[2], np.float32)
+        if L.ref_pulse_sparse(h, self.freq_it0.ctypes.data, self.freq_nt.ctypes.data, self.freq_sd_off.ctypes.data,
+                              self.sparse_data.ctypes.data) != 0:
+            raise RuntimeError(_err())
+
+    def add_to_timestream(self, out, out_it0, weight=1.0):
+        assert out.dtype == np.float32 and out.flags.c_contiguous and out.ndim == 2
+        if lib().ref_pulse_add_to_timestream(self.h, out.ctypes.data, out.shape[0], out.shape[1], int(out_it0),
+                                             float(weight)) != 0:
+            raise RuntimeError("pirate SinglePulse.add_to_timestream: " + _err())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ref_pulse_destroy(self.h)
+            self.h = None

@@ -33,7 +33,9 @@ CASES = H.pirate_fixture_cases()
 
 def test_fixture_covers_every_case():
     _, meta = _fixtures()
-    assert sorted(meta) == sorted(c["name"] for c in CASES)
+    ded = sorted(k for k, v in meta.items() if v.get("kind") != "pulse")
+    assert ded == sorted(c["name"] for c in CASES)
+    assert sorted(k for k, v in meta.items() if v.get("kind") == "pulse") == sorted(c["name"] for c in H.pulse_fixture_cases())
     # The small cases were also checked equal across pirate's three reference sophistications.
     assert all(meta[c["name"]]["sophistication_equal"] == [0, 2] for c in CASES if c["cfg"]["toplevel_tree_rank"] <= 12)
 

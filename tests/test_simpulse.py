@@ -153,3 +153,26 @@ def test_subband_and_errors(pb2lib):
     for b in bad:
         with pytest.raises(RuntimeError):
             sp.SinglePulse(**b)
+
+
+def test_matches_pirate_simpulse(pb2lib):
+    """Against pirate's own SinglePulse (src_lib/simpulse.cpp compiled unmodified in oracle/_ref, MKL's
+    complex-to-real DFT supplied by oracle/ksgpu_shim/mkl_dfti.h), committed by
+    tests/golden/make_ref_golden.py: the same sample ranges exactly, and the same float32 samples to
+    within 1e-6 of the pulse's peak (they agree bit for bit when generated)."""
+    import json
+    import os
+    import helpers as H
+    fix = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "pirate_ref_fixtures.npz"))
+    meta = json.loads(bytes(fix["meta_json"]).decode())
+    sp_mod = _sp()
+    for pc in H.pulse_fixture_cases():
+        m = meta[pc["name"]]
+        sp = sp_mod.SinglePulse(freq_edges_MHz=pc["edges"], freq_variances=pc["var"], **pc["params"])
+        assert (sp.it_start, sp.it_end) == (m["it_start"], m["it_end"]), pc["name"]
+        for k in ("freq_it0", "freq_nt", "freq_sd_off"):
+            assert np.array_equal(getattr(sp, k), fix["%s/%s" % (pc["name"], k)]), (pc["name"], k)
+        ref = fix["%s/sparse_data" % pc["name"]]
+        assert sp.sparse_data.shape == ref.shape
+        err = np.abs(sp.sparse_data.astype(np.float64) - ref).max()
+        assert err <= 1e-6 * np.abs(ref).max(), (pc["name"], err)
