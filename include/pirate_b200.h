@@ -214,6 +214,10 @@ int pb2_dd_fill_weights(pb2_dedisperser *dd, long itree, const float *host, long
 int pb2_dd_fill_analytic_weights(pb2_dedisperser *dd, const double *freq_variances, long nfreq);
 /* GpuDedisperser::stop, src_lib/GpuDedisperser.cpp:735 */
 int pb2_dd_stop(pb2_dedisperser *dd);
+/* Clears every delay line and tree state (and the input and output slots) on 'stream', after waiting for
+ * the batches already launched: later chunks see zeros as their history, as at the start of a stream.
+ * The seq_id cursors are unchanged. (No pirate counterpart; used to separate synthetic events.) */
+int pb2_dd_zero_state(pb2_dedisperser *dd, void *stream);
 /* Kernel launches per (chunk, batch), and algorithmic HBM bytes per (chunk, batch) for the
  * kernel classes [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf]. */
 int pb2_dd_kernels_per_batch(const pb2_dedisperser *dd, long *n);
@@ -253,6 +257,34 @@ int pb2_sifter_train_step(pb2_sifter *s, const void *patches, const float *label
  * peaks). The results appear in pb2_outputs. The sifter then runs on the dedisperser's compute stream
  * and must neither be trained meanwhile nor destroyed before the dedisperser. */
 int pb2_dd_enable_sifter(pb2_dedisperser *dd, float threshold, pb2_sifter *sifter);
+
+/* ---- Many beams with uneven plans, one CUDA graph per chunk (pirate: one GpuDedisperser per plan on a
+ * pool of compute streams, src_lib/GpuDedisperser.cpp:990-1000) ----
+ *
+ * One group per plan; each group's beams form one batch (beams_per_gpu == beams_per_batch). A step is
+ * one chunk of every group, run as one replayed CUDA graph whose kernels read the chunk index from a
+ * device counter. Inputs: the group's input slot (pb2_batched_input) written before the step, on the
+ * step's stream or ordered before it; outputs (pb2_batched_outputs, no candidate arrays) valid after it.
+ * pb2_batched_autotune times the schedule choices (per group: merged stage-2 grids, peak-finder
+ * variant, gridding block size; branch concurrency), keeps the fastest, clears the state and writes a
+ * JSON record of the trials (copy_out convention of pb2_config_to_yaml). */
+typedef struct pb2_batched pb2_batched;
+int pb2_batched_create(const pb2_plan *const *plans, long nplans, int cuda_device_id, pb2_batched **out);
+int pb2_batched_allocate(pb2_batched *b);
+int pb2_batched_ngroups(const pb2_batched *b, long *n);
+int pb2_batched_device_bytes(const pb2_batched *b, long *nbytes);
+int pb2_batched_fill_weights(pb2_batched *b, long group, long itree, const float *host, long nelts);
+int pb2_batched_fill_analytic_weights(pb2_batched *b, long group, const double *freq_variances, long nfreq);
+int pb2_batched_input(pb2_batched *b, long group, void **ptr, long *shape3);
+int pb2_batched_outputs(pb2_batched *b, long group, pb2_outputs *out);
+int pb2_batched_step(pb2_batched *b, void *stream);
+int pb2_batched_reset(pb2_batched *b, void *stream);
+int pb2_batched_set_schedule(pb2_batched *b, const int *merge_stage2, const int *pf_general, const int *grid_block,
+                             int concurrent);
+int pb2_batched_autotune(pb2_batched *b, int reps, char *buf, long buflen, long *needed);
+int pb2_batched_time_steps(pb2_batched *b, int nsteps, void *stream, double *ms_per_step);
+int pb2_batched_kernels_per_step(const pb2_batched *b, long *n);
+void pb2_batched_destroy(pb2_batched *b);
 
 /* ---- Allocation-free single-chunk dedispersion (no counterpart in pirate) ----
  *

@@ -112,6 +112,22 @@ def lib():
         "pb2_sifter_gradients": (ctypes.c_int, [vp, vp, vp, ctypes.c_long, vp, dp, vp]),
         "pb2_sifter_train_step": (ctypes.c_int, [vp, vp, vp, ctypes.c_long, ctypes.c_float, dp, vp]),
         "pb2_dd_enable_sifter": (ctypes.c_int, [vp, ctypes.c_float, vp]),
+        "pb2_dd_zero_state": (ctypes.c_int, [vp, vp]),
+        "pb2_batched_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_long, ctypes.c_int, ctypes.POINTER(vp)]),
+        "pb2_batched_allocate": (ctypes.c_int, [vp]),
+        "pb2_batched_ngroups": (ctypes.c_int, [vp, lp]),
+        "pb2_batched_device_bytes": (ctypes.c_int, [vp, lp]),
+        "pb2_batched_fill_weights": (ctypes.c_int, [vp, ctypes.c_long, ctypes.c_long, vp, ctypes.c_long]),
+        "pb2_batched_fill_analytic_weights": (ctypes.c_int, [vp, ctypes.c_long, dp, ctypes.c_long]),
+        "pb2_batched_input": (ctypes.c_int, [vp, ctypes.c_long, ctypes.POINTER(vp), lp]),
+        "pb2_batched_outputs": (ctypes.c_int, [vp, ctypes.c_long, ctypes.POINTER(_Outputs)]),
+        "pb2_batched_step": (ctypes.c_int, [vp, vp]),
+        "pb2_batched_reset": (ctypes.c_int, [vp, vp]),
+        "pb2_batched_set_schedule": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
+        "pb2_batched_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_long, lp]),
+        "pb2_batched_time_steps": (ctypes.c_int, [vp, ctypes.c_int, vp, dp]),
+        "pb2_batched_kernels_per_step": (ctypes.c_int, [vp, lp]),
+        "pb2_batched_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -497,6 +513,11 @@ class GpuDedisperser:
     def stop(self):
         _check(lib().pb2_dd_stop(self._h))
 
+    def zero_state(self, stream=None):
+        """Clears every delay line and tree state (later chunks see zeros as history); the seq_id
+        cursors are unchanged."""
+        _check(lib().pb2_dd_zero_state(self._h, _stream_ptr(stream)))
+
     def enable_sifter(self, threshold=6.0, sifter=None):
         """Adds the candidate stage to every later batch: each beam's strongest output over the trees,
         the fp16 patch (9 DM x 32 time x 6 width) of peaks >= threshold, and its score by 'sifter'
@@ -537,6 +558,91 @@ class GpuDedisperser:
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.pb2_dd_destroy(self._h)
+            self._h = None
+
+
+class BatchedDedisperser:
+    """Many beams with uneven plans (tree rank, primary trees), one group per plan, each group's beams
+    one batch; step() runs one chunk of every group as one replayed CUDA graph (include/pirate_b200.h,
+    pb2_batched_*). pirate's counterpart is one GpuDedisperser per plan on a pool of compute streams
+    (src_lib/GpuDedisperser.cpp:990-1000)."""
+
+    def __init__(self, plans, cuda_device_id=0):
+        self.plans = list(plans)
+        self.device = "cuda:%d" % int(cuda_device_id)
+        arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value if hasattr(p._h, "value") else p._h for p in self.plans])
+        h = ctypes.c_void_p()
+        _check(lib().pb2_batched_create(arr, len(self.plans), int(cuda_device_id), ctypes.byref(h)))
+        self._h = h
+
+    def allocate(self):
+        _check(lib().pb2_batched_allocate(self._h))
+
+    @property
+    def ngroups(self):
+        return len(self.plans)
+
+    def device_bytes(self):
+        n = ctypes.c_long()
+        _check(lib().pb2_batched_device_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def fill_all_weights(self, group, itree, pf_weights):
+        """pf_weights: (1, beams, ndm_wt, nt_wt, nprofiles, N) float32 (one weight slot)."""
+        w = np.ascontiguousarray(pf_weights, dtype=np.float32)
+        _check(lib().pb2_batched_fill_weights(self._h, int(group), int(itree), w.ctypes.data, w.size))
+
+    def fill_analytic_weights(self, group, freq_variances):
+        fv = np.ascontiguousarray(freq_variances, dtype=np.float64)
+        _check(lib().pb2_batched_fill_analytic_weights(self._h, int(group), fv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), fv.size))
+
+    def input(self, group):
+        """The group's input slot, a (beams, nfreq, nt_in) CUDA tensor view in the plan's dtype."""
+        ptr = ctypes.c_void_p()
+        shape = (ctypes.c_long * 3)()
+        _check(lib().pb2_batched_input(self._h, int(group), ctypes.byref(ptr), shape))
+        return _device_tensor(ptr.value, tuple(shape), self.plans[group].dtype, self.device)
+
+    def outputs(self, group):
+        o = _Outputs()
+        _check(lib().pb2_batched_outputs(self._h, int(group), ctypes.byref(o)))
+        return Outputs(o, self.device)
+
+    def step(self, stream=None):
+        _check(lib().pb2_batched_step(self._h, _stream_ptr(stream)))
+
+    def reset(self, stream=None):
+        _check(lib().pb2_batched_reset(self._h, _stream_ptr(stream)))
+
+    def set_schedule(self, merge_stage2, pf_general, grid_block, concurrent=True):
+        n = self.ngroups
+        m = (ctypes.c_int * n)(*[int(bool(x)) for x in merge_stage2])
+        p = (ctypes.c_int * n)(*[int(bool(x)) for x in pf_general])
+        g = (ctypes.c_int * n)(*[int(x) for x in grid_block])
+        _check(lib().pb2_batched_set_schedule(self._h, m, p, g, int(bool(concurrent))))
+
+    def autotune(self, reps=5):
+        """Times the schedule choices on the replayed graph, keeps the fastest, clears the state;
+        returns the record of trials and the choice (dict)."""
+        import json
+        n = ctypes.c_long()
+        buf = ctypes.create_string_buffer(1 << 16)
+        _check(lib().pb2_batched_autotune(self._h, int(reps), buf, len(buf), ctypes.byref(n)))
+        return json.loads(buf.value.decode())
+
+    def time_steps(self, n, stream=None):
+        ms = ctypes.c_double()
+        _check(lib().pb2_batched_time_steps(self._h, int(n), _stream_ptr(stream), ctypes.byref(ms)))
+        return ms.value
+
+    def kernels_per_step(self):
+        n = ctypes.c_long()
+        _check(lib().pb2_batched_kernels_per_step(self._h, ctypes.byref(n)))
+        return n.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pb2_batched_destroy(self._h)
             self._h = None
 
 

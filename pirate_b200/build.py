@@ -13,8 +13,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpirate_b200.so")
 
-SOURCES = ["plan.cpp", "avar.cpp", "simpulse.cpp", "capi.cpp", "kernels.cu", "dedisperser.cu", "noalloc.cu", "sifter.cu"]
-HEADERS = ["plan.hpp", "avar.hpp", "simpulse.hpp", "yaml_lite.hpp", "kernels.cuh", "dedisperser.hpp", "regtree.cuh", "sifter.hpp"]
+SOURCES = ["plan.cpp", "avar.cpp", "simpulse.cpp", "capi.cpp", "kernels.cu", "dedisperser.cu", "noalloc.cu", "sifter.cu", "batched.cu"]
+HEADERS = ["plan.hpp", "avar.hpp", "simpulse.hpp", "yaml_lite.hpp", "kernels.cuh", "dedisperser.hpp", "regtree.cuh", "sifter.hpp", "batched.hpp"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

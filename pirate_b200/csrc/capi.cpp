@@ -7,6 +7,7 @@
 #include "kernels.cuh"
 #include "simpulse.hpp"
 #include "sifter.hpp"
+#include "batched.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -20,6 +21,32 @@ struct pb2_config { DedispersionConfig c; };
 struct pb2_plan { std::shared_ptr<DedispersionPlan> p; };
 struct pb2_dedisperser { std::unique_ptr<GpuDedisperser> d; };
 struct pb2_sifter { std::unique_ptr<Sifter> s; };
+struct pb2_batched { std::unique_ptr<BatchedDedisperser> b; };
+
+static void fill_outputs(const GpuDedisperser::Outputs &o, pb2_outputs *out)
+{
+    memset(out, 0, sizeof(*out));
+    out->dtype = int(o.dtype);
+    out->nbeams = o.nbeams;
+    out->ichunk_zero_based = o.ichunk_zero_based;
+    out->ichunk_fpga_based = o.ichunk_fpga_based;
+    out->ibeam = o.ibeam;
+    out->ntrees = long(o.out_max.size());
+    for (size_t i = 0; i < o.out_max.size(); i++) {
+        out->ndm_out[i] = o.ndm_out[i];
+        out->nt_out[i] = o.nt_out[i];
+        out->out_max[i] = o.out_max[i];
+        out->out_argmax[i] = o.out_argmax[i];
+    }
+    out->cand_peak = o.cand_peak;
+    out->cand_tree = o.cand_tree;
+    out->cand_idm = o.cand_idm;
+    out->cand_itime = o.cand_itime;
+    out->cand_valid = o.cand_valid;
+    out->cand_token = o.cand_token;
+    out->patches = o.patches;
+    out->scores = o.scores;
+}
 
 #define CUDA_CHECK(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) \
     throw std::runtime_error(std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
@@ -487,6 +514,11 @@ int pb2_dd_stop(pb2_dedisperser *dd)
     return guard([&] { REQUIRE_PTR(dd); dd->d->stop(); });
 }
 
+int pb2_dd_zero_state(pb2_dedisperser *dd, void *stream)
+{
+    return guard([&] { REQUIRE_PTR(dd); dd->d->zero_state((cudaStream_t) stream); });
+}
+
 int pb2_dd_kernels_per_batch(const pb2_dedisperser *dd, long *n)
 {
     return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(n); *n = dd->d->kernels_per_batch(); });
@@ -566,6 +598,107 @@ int pb2_dd_enable_sifter(pb2_dedisperser *dd, float threshold, pb2_sifter *sifte
 {
     return guard([&] { REQUIRE_PTR(dd); dd->d->enable_sifter(threshold, sifter ? sifter->s.get() : nullptr); });
 }
+
+int pb2_batched_create(const pb2_plan *const *plans, long nplans, int cuda_device_id, pb2_batched **out)
+{
+    return guard([&] {
+        REQUIRE_PTR(plans); REQUIRE_PTR(out);
+        if (nplans < 1) throw std::runtime_error("pb2_batched_create: no plans");
+        std::vector<DedispersionPlan> ps;
+        for (long i = 0; i < nplans; i++) {
+            REQUIRE_PTR(plans[i]);
+            if (plans[i]->p->ntrees > PB2_MAX_TREES) throw std::runtime_error("pb2_batched_create: too many trees");
+            ps.push_back(*plans[i]->p);
+        }
+        *out = new pb2_batched{std::unique_ptr<BatchedDedisperser>(new BatchedDedisperser(ps, cuda_device_id))};
+    });
+}
+
+int pb2_batched_allocate(pb2_batched *b) { return guard([&] { REQUIRE_PTR(b); b->b->allocate(); }); }
+
+int pb2_batched_ngroups(const pb2_batched *b, long *n)
+{
+    return guard([&] { REQUIRE_PTR(b); REQUIRE_PTR(n); *n = b->b->ngroups(); });
+}
+
+int pb2_batched_device_bytes(const pb2_batched *b, long *nbytes)
+{
+    return guard([&] {
+        REQUIRE_PTR(b); REQUIRE_PTR(nbytes);
+        long t = 0;
+        for (long g = 0; g < b->b->ngroups(); g++) t += long(b->b->group(g).device_bytes());
+        *nbytes = t;
+    });
+}
+
+int pb2_batched_fill_weights(pb2_batched *b, long group, long itree, const float *host, long nelts)
+{
+    return guard([&] { REQUIRE_PTR(b); REQUIRE_PTR(host); b->b->group(group).fill_all_weights(itree, host, nelts); });
+}
+
+int pb2_batched_fill_analytic_weights(pb2_batched *b, long group, const double *freq_variances, long nfreq)
+{
+    return guard([&] { REQUIRE_PTR(b); REQUIRE_PTR(freq_variances); b->b->group(group).fill_analytic_weights(freq_variances, nfreq); });
+}
+
+int pb2_batched_input(pb2_batched *b, long group, void **ptr, long *shape3)
+{
+    return guard([&] {
+        REQUIRE_PTR(b); REQUIRE_PTR(ptr); REQUIRE_PTR(shape3);
+        GpuDedisperser &g = b->b->group(group);
+        *ptr = g.input_ptr(0);
+        shape3[0] = g.plan.beams_per_batch;
+        shape3[1] = g.plan.nfreq;
+        shape3[2] = g.plan.nt_in;
+    });
+}
+
+int pb2_batched_outputs(pb2_batched *b, long group, pb2_outputs *out)
+{
+    return guard([&] {
+        REQUIRE_PTR(b); REQUIRE_PTR(out);
+        GpuDedisperser::Outputs o = b->b->group(group).outputs_ptr(0);
+        o.ichunk_zero_based = b->b->chunks_done() - 1;
+        o.ichunk_fpga_based = o.ichunk_zero_based;
+        fill_outputs(o, out);
+    });
+}
+
+int pb2_batched_step(pb2_batched *b, void *stream) { return guard([&] { REQUIRE_PTR(b); b->b->step((cudaStream_t) stream); }); }
+
+int pb2_batched_reset(pb2_batched *b, void *stream) { return guard([&] { REQUIRE_PTR(b); b->b->reset((cudaStream_t) stream); }); }
+
+int pb2_batched_set_schedule(pb2_batched *b, const int *merge_stage2, const int *pf_general, const int *grid_block,
+                             int concurrent)
+{
+    return guard([&] {
+        REQUIRE_PTR(b); REQUIRE_PTR(merge_stage2); REQUIRE_PTR(pf_general); REQUIRE_PTR(grid_block);
+        std::vector<GroupTuning> t(b->b->ngroups());
+        for (size_t g = 0; g < t.size(); g++) {
+            t[g].merge_stage2 = merge_stage2[g] != 0;
+            t[g].pf_general = pf_general[g] != 0;
+            t[g].grid_block = grid_block[g];
+        }
+        b->b->set_schedule(t, concurrent != 0);
+    });
+}
+
+int pb2_batched_autotune(pb2_batched *b, int reps, char *buf, long buflen, long *needed)
+{
+    return guard([&] { REQUIRE_PTR(b); copy_out(b->b->autotune(reps), buf, buflen, needed); });
+}
+
+int pb2_batched_time_steps(pb2_batched *b, int nsteps, void *stream, double *ms_per_step)
+{
+    return guard([&] { REQUIRE_PTR(b); REQUIRE_PTR(ms_per_step); *ms_per_step = b->b->time_steps(nsteps, (cudaStream_t) stream); });
+}
+
+int pb2_batched_kernels_per_step(const pb2_batched *b, long *n)
+{
+    return guard([&] { REQUIRE_PTR(b); REQUIRE_PTR(n); *n = b->b->kernels_per_step(); });
+}
+
+void pb2_batched_destroy(pb2_batched *b) { delete b; }
 
 int pb2_dedisperse_chunk_noalloc(const pb2_plan *plan, const void *in, const float *const *weights,
                                  void *const *out_max, uint32_t *const *out_argmax, void *stream)

@@ -469,11 +469,63 @@ void GpuDedisperser::release_input_and_launch_dd_kernels(long seq_id, cudaStream
 void GpuDedisperser::launch_batch(long seq_id)
 {
     const long ichunk = seq_id / nbatches, ibatch = seq_id % nbatches;
-    const long slot_in = seq_id % nslots_in, slot_out = seq_id % nbatches_out, slot_wt = seq_id % nbatches_wt;
+    launch_kernels(ichunk, ibatch, seq_id % nslots_in, seq_id % nbatches_out, seq_id % nbatches_wt, compute, nullptr,
+                   GroupTuning(), true);
+}
+
+void GpuDedisperser::enqueue_chunk(cudaStream_t stream, const long *chunk_ctr, const GroupTuning &tune)
+{
+    entry([&]() {
+        if (!allocated) throw runtime_error("GpuDedisperser::enqueue_chunk(): allocate() was not called");
+        if (nbatches != 1) throw runtime_error("GpuDedisperser::enqueue_chunk(): needs beams_per_gpu == beams_per_batch");
+        if (!chunk_ctr) throw runtime_error("GpuDedisperser::enqueue_chunk(): null chunk counter");
+        launch_kernels(0, 0, 0, 0, 0, stream, chunk_ctr, tune, false);
+    });
+}
+
+void *GpuDedisperser::input_ptr(long slot) const
+{
+    if (slot < 0 || slot >= nslots_in || !allocated) throw runtime_error("GpuDedisperser::input_ptr(): bad slot");
+    return d_inputs.as<char>() + size_t(slot) * B * plan.nfreq * plan.nt_in * esize;
+}
+
+GpuDedisperser::Outputs GpuDedisperser::outputs_ptr(long slot) const
+{
+    if (slot < 0 || slot >= nbatches_out || !allocated) throw runtime_error("GpuDedisperser::outputs_ptr(): bad slot");
+    Outputs o;
+    o.dtype = plan.dtype;
+    o.nbeams = B;
+    for (long i = 0; i < plan.ntrees; i++) {
+        const DedispersionTree &t = plan.trees[i];
+        size_t osz = size_t(B) * t.ndm_out * t.nt_out;
+        o.ndm_out.push_back(t.ndm_out);
+        o.nt_out.push_back(t.nt_out);
+        o.out_max.push_back(s2[i].out_max.as<char>() + size_t(slot) * osz * esize);
+        o.out_argmax.push_back(s2[i].out_argmax.as<uint32_t>() + size_t(slot) * osz);
+    }
+    return o;
+}
+
+void GpuDedisperser::zero_state(cudaStream_t s)
+{
+    entry([&]() {
+        if (!allocated) throw runtime_error("GpuDedisperser::zero_state(): allocate() was not called");
+        CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
+        CUDA_CHECK(cudaStreamSynchronize(compute));   // no batch of this object may still be running
+        auto z = [&](const DeviceBuffer &d) { if (d.ptr) CUDA_CHECK(cudaMemsetAsync(d.ptr, 0, d.nbytes, s)); };
+        z(d_inputs); z(d_tree0); z(d_lds_state); z(d_qdata); z(d_qscoff); z(d_cand); z(d_patches);
+        for (auto &st : s1) { z(st.ring); z(st.state); z(st.lds); }
+        for (auto &st : s2) { z(st.state); z(st.pfring); z(st.out_max); z(st.out_argmax); }
+    });
+}
+
+void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long slot_out, long slot_wt, cudaStream_t s,
+                                    const long *ctr, const GroupTuning &tune, bool fences)
+{
     const long rank = plan.config.toplevel_tree_rank, nt = plan.nt_in, F = plan.nfreq, N = pow2(rank);
     const long npri = plan.num_primary_trees;
     const int beam0 = int(ibatch * B);
-    cudaStream_t s = compute;
+    const bool tk = (ctr == nullptr);   // kernel timing ticks only on the compute stream
 
     GridLdsArgs g;
     memset(&g, 0, sizeof(g));
@@ -495,12 +547,16 @@ void GpuDedisperser::launch_batch(long seq_id)
     g.state = d_lds_state.as<float>();
     g.lag_rank = (npri > 1) ? int(plan.stage1_dd_rank[1]) : 0;
     g.ichunk = ichunk;
+    g.chunk_ctr = ctr;
+    g.block_target = tune.grid_block;
     g.beam0 = beam0; g.B = int(B); g.total_beams = int(total_beams);
-    cudaEvent_t t0 = tick(0, nullptr);
+    cudaEvent_t t0 = tk ? tick(0, nullptr) : nullptr;
     launch_grid_lds(g, dtype_code, s);
-    tick(0, t0);
-    CUDA_CHECK(cudaEventRecord(ev_in_free[slot_in], s));
-    in_free_recorded[slot_in] = true;
+    if (tk) tick(0, t0);
+    if (fences) {
+        CUDA_CHECK(cudaEventRecord(ev_in_free[slot_in], s));
+        in_free_recorded[slot_in] = true;
+    }
 
     for (long p = 0; p < npri; p++) {
         Stage1 &st = s1[p];
@@ -533,9 +589,10 @@ void GpuDedisperser::launch_batch(long seq_id)
         a.s0 = ichunk * st.nt;
         a.nt = st.nt;
         a.beam0 = beam0;
-        cudaEvent_t t2 = tick(2, nullptr);
+        a.chunk_ctr = ctr;
+        cudaEvent_t t2 = tk ? tick(2, nullptr) : nullptr;
         launch_stage1(a, dtype_code, st.nblocks, int(B), s);
-        tick(2, t2);
+        if (tk) tick(2, t2);
     }
 
     std::vector<Stage2Args> a2(plan.ntrees);
@@ -563,22 +620,24 @@ void GpuDedisperser::launch_batch(long seq_id)
         a.s0 = ichunk * t.nt_ds;
         a.nt = t.nt_ds;
         a.beam0 = beam0;
+        a.chunk_ctr = ctr;
         nb2[i] = int(st.nblocks);
     }
     // Consecutive output trees that use the same stage-2 kernel share one launch.
     for (long i0 = 0; i0 < plan.ntrees;) {
         long i1 = i0 + 1;
-        while (i1 < plan.ntrees && i1 - i0 < kStage2MaxTrees && stage2_same_kernel(a2[i0], a2[i1])) i1++;
-        cudaEvent_t t3 = tick(3, nullptr);
+        while (tune.merge_stage2 && i1 < plan.ntrees && i1 - i0 < kStage2MaxTrees && stage2_same_kernel(a2[i0], a2[i1])) i1++;
+        cudaEvent_t t3 = tk ? tick(3, nullptr) : nullptr;
         launch_stage2_multi(&a2[i0], &nb2[i0], int(i1 - i0), dtype_code, int(B), s);
-        tick(3, t3);
+        if (tk) tick(3, t3);
         i0 = i1;
     }
 
     // Output back-pressure: slot_out is reusable once every consumer released seq_id - nbatches_out.
-    for (long c = 0; c < params.num_consumers; c++)
-        if (out_released_recorded[c][slot_out])
-            CUDA_CHECK(cudaStreamWaitEvent(s, ev_out_released[c][slot_out], 0));
+    if (fences)
+        for (long c = 0; c < params.num_consumers; c++)
+            if (out_released_recorded[c][slot_out])
+                CUDA_CHECK(cudaStreamWaitEvent(s, ev_out_released[c][slot_out], 0));
 
     for (long i = 0; i < plan.ntrees; i++) {
         const DedispersionTree &t = plan.trees[i];
@@ -599,13 +658,16 @@ void GpuDedisperser::launch_batch(long seq_id)
         a.Dout = st.Dout; a.Dcore = int(t.Dcore); a.tpad = st.tpad;
         a.s0 = ichunk * t.nt_ds;
         a.beam0 = beam0;
-        cudaEvent_t t4 = tick(4, nullptr);
+        a.chunk_ctr = ctr;
+        a.nt_chunk = int(t.nt_ds);
+        a.force_general = tune.pf_general ? 1 : 0;
+        cudaEvent_t t4 = tk ? tick(4, nullptr) : nullptr;
         launch_pf(a, dtype_code, int(B), s);
-        tick(4, t4);
+        if (tk) tick(4, t4);
     }
     if (sift) {
         // Candidate stage: per-beam peak over the trees, patches of the peaks >= threshold, scores.
-        cudaEvent_t t1 = tick(1, nullptr);
+        cudaEvent_t t1 = tk ? tick(1, nullptr) : nullptr;
         float *cb = (float *) d_cand.ptr + size_t(slot_out) * 8 * B;
         BeamPeakArgs ba;
         memset(&ba, 0, sizeof(ba));
@@ -632,6 +694,7 @@ void GpuDedisperser::launch_batch(long seq_id)
         pa.peak = ba.peak; pa.tree = ba.tree; pa.idm = ba.idm; pa.itime = ba.itime; pa.token = ba.token;
         pa.valid = (int *) (cb + 5 * B);
         pa.ichunk = ichunk;
+        pa.chunk_ctr = ctr;
         pa.beam0 = beam0;
         pa.patches = d_patches.as<uint16_t>() + size_t(slot_out) * B * kPatchLen;
         launch_patches(pa, dtype_code, s);
@@ -642,10 +705,12 @@ void GpuDedisperser::launch_batch(long seq_id)
         } else {
             launch_mask_scores(ba.peak, pa.valid, scores, int(B), s);
         }
-        tick(1, t1);
+        if (tk) tick(1, t1);
     }
-    CUDA_CHECK(cudaEventRecord(ev_out_done[slot_out], s));
-    out_done_recorded[slot_out] = true;
+    if (fences) {
+        CUDA_CHECK(cudaEventRecord(ev_out_done[slot_out], s));
+        out_done_recorded[slot_out] = true;
+    }
 }
 
 GpuDedisperser::Outputs GpuDedisperser::acquire_output(long consumer_id, long seq_id, cudaStream_t stream, bool sync)

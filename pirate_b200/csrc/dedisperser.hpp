@@ -44,6 +44,14 @@ struct DeviceBuffer
     template<typename T> T *as() const { return (T *) ptr; }
 };
 
+// Schedule knobs of one dedisperser's kernel sequence (chosen per plan by BatchedDedisperser::autotune).
+struct GroupTuning
+{
+    bool merge_stage2 = true;   // one stage-2 grid for consecutive trees with the same kernel
+    bool pf_general = false;    // the general peak-finding kernel even where the fast one applies
+    int grid_block = 128;       // threads per gridding block (a multiple of the windows per row; <= 512)
+};
+
 class GpuDedisperser
 {
 public:
@@ -106,6 +114,17 @@ public:
     // enable_sifter() call.
     void enable_sifter(float threshold, Sifter *sifter);
 
+    // Batched use (BatchedDedisperser): enqueues one chunk of the single batch (needs beams_per_gpu ==
+    // beams_per_batch) on 'stream', every kernel reading the chunk index from the device counter
+    // *chunk_ctr; input slot 0, output slot 0, weight slot 0; no events and no back-pressure (the caller
+    // orders the chunks). It makes no host-side waits, so it can be captured in a CUDA graph.
+    void enqueue_chunk(cudaStream_t stream, const long *chunk_ctr, const GroupTuning &tune);
+    void *input_ptr(long slot) const;
+    Outputs outputs_ptr(long slot) const;
+    // Clears every delay line, tree state, input and output slot on 'stream' (a fresh stream of chunks:
+    // later chunks see zeros as their history). Waits for this object's launched batches first.
+    void zero_state(cudaStream_t stream);
+
     // Device bytes held by allocate() (for reporting).
     size_t device_bytes() const { return total_bytes; }
     // Number of kernels launched per (chunk, batch).
@@ -130,6 +149,8 @@ private:
     void check_alive() const;
     template<typename F> auto entry(F &&f) -> decltype(f());
     void launch_batch(long seq_id);
+    void launch_kernels(long ichunk, long ibatch, long slot_in, long slot_out, long slot_wt, cudaStream_t s,
+                        const long *chunk_ctr, const GroupTuning &tune, bool fences);
 
     std::mutex mtx;
     std::condition_variable cv;                     // signalled by release_output() and stop()

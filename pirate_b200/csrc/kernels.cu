@@ -17,6 +17,7 @@
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -437,7 +438,8 @@ __global__ void __launch_bounds__(kGridMaxThreads) grid_lds_kernel(GridLdsArgs a
     const long c = (gg / nwin) % nhalf;
     const int b = int(gg / (nwin * nhalf));
     const int bt = a.beam0 + b;
-    const int parity = int(a.ichunk & 1);
+    const long ichunk = a.chunk_ctr ? *a.chunk_ctr : a.ichunk;
+    const int parity = int(ichunk & 1);
     const long t0 = (long) win * W0;
 
     float r0[W0], r1[W0];
@@ -473,7 +475,7 @@ __global__ void __launch_bounds__(kGridMaxThreads) grid_lds_kernel(GridLdsArgs a
                 const long cap = a.cap_mask[p - 1] + 1;
                 Ts *ring = (Ts *) a.ring[p - 1] + ((long) bt * nhalf + c) * cap;
                 const long nt_p = a.T >> p;
-                const long s_base = a.ichunk * nt_p + (long) win * len + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
+                const long s_base = ichunk * nt_p + (long) win * len + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
 #pragma unroll
                 for (int u = 1; u < (W0 >> 1); u++)
                     if (u < len)
@@ -511,7 +513,7 @@ __global__ void __launch_bounds__(kGridMaxThreads) grid_lds_kernel(GridLdsArgs a
                 const long cap = a.cap_mask[p - 1] + 1;
                 Ts *ring = (Ts *) a.ring[p - 1] + ((long) bt * nhalf + c) * cap;
                 const long nt_p = a.T >> p;
-                const long s_base = a.ichunk * nt_p + (long) win * (W0 >> p) + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
+                const long s_base = ichunk * nt_p + (long) win * (W0 >> p) + ((1L << a.lag_rank) - 1 - (c & ((1L << a.lag_rank) - 1)));
                 ring[s_base & a.cap_mask[p - 1]] = from_f<Ts>(bfly(prev[p - 1], first[p - 1]));
             }
         }
@@ -964,13 +966,14 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(c
         for (int i = threadIdx.x; i < RING; i += blockDim.x)
             ring[i] = st[i];
     }
-    ring_init<RA, RB>(wb, rt, in_cap, a.s0);
+    const long s0 = a.chunk_ctr ? *a.chunk_ctr * (long) a.nt : a.s0;
+    ring_init<RA, RB>(wb, rt, in_cap, s0);
 
     const Ts *in;
     int pos1 = 0;   // stage 1: read position of every input row (rows are read aligned)
     if constexpr (STAGE == 1) {
         in = (const Ts *) a.in + (long) (a.in_beam0 + b) * a.in_beam_stride + (long) blk * NR * a.in_row_stride;
-        pos1 = int(a.in_s0 & a.in_mask);
+        pos1 = int(((a.chunk_ctr && a.in_mask != -1) ? s0 : a.in_s0) & a.in_mask);
         const long off0 = a.ring_off[(long) blk * NR];   // the host checks that a block's lines span < 2^31
         for (int r = threadIdx.x; r < NR; r += blockDim.x) {
             const int cap = a.ring_cap[(long) blk * NR + r];   // capacity of output delay line r (a multiple of 32)
@@ -978,7 +981,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(c
             const int j = (r & (NA - 1)) * NB + (r >> RA);      // row (f, d) = r at [d * NB + f]
             in_cap[j] = cap;
             out_off[j] = off;
-            out_base[j] = off + int(a.s0 % cap);
+            out_base[j] = off + int(s0 % cap);
         }
     } else {
         in = (const Ts *) a.ring + (long) bt * a.ring_beam_stride;
@@ -987,7 +990,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(c
             long row = ((long) r << a.amb_rank) + blk;
             long lag = (long) (NR - 1 - r) * dm1;
             long cap = a.ring_cap[row];
-            long p = (a.s0 - lag) % cap;
+            long p = (s0 - lag) % cap;
             const long off = a.ring_off[row];
             in_tab[r] = make_int4(int(p < 0 ? p + cap : p), int(cap), int(off & 0xffffffffL), int(off >> 32));
         }
@@ -1134,7 +1137,7 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(c
             const int pf_dm = brev_bits(g, RA);
             const long rowbase = ((long) bt * a.ndm_out + ((long) brev_bits(blk, a.amb_rank) << RA) + pf_dm) * a.M;
             pf_rows = (Ts *) a.pf + rowbase * a.pf_cap;
-            pf_slot = int((a.s0 + lane) & (a.pf_cap - 1));
+            pf_slot = int((s0 + lane) & (a.pf_cap - 1));
             emit.cap = int(a.pf_cap);
         }
 
@@ -1322,6 +1325,7 @@ __device__ __forceinline__ void pf_group(const float *x, int nsamp, int S, float
 template<typename Ts, int L>
 __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_floats)
 {
+    const long s0 = a.chunk_ctr ? *a.chunk_ctr * (long) a.nt_chunk : a.s0;
     extern __shared__ float sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int dm = blockIdx.y * kPfWarps + warp;
@@ -1340,7 +1344,7 @@ __global__ void __launch_bounds__(kPfWarps * 32) pf_kernel(PfArgs a, int warp_fl
     const float *wp = a.wt + ((((long) b * a.ndm_wt + dm / Wds) * a.nt_wt + (active ? tout / Tds : 0)) * a.P) * a.N;
     const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
     const long mask = a.pf_cap - 1;
-    const long s_base = a.s0 + (long) tout0 * a.Dout - a.tpad;
+    const long s_base = s0 + (long) tout0 * a.Dout - a.tpad;
     const bool full = (a.P > 1);
 
     float best = -1.0e30f;
@@ -1570,7 +1574,8 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
     const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
     const int mask = int(a.pf_cap - 1);
     // Window sample 0 (stream time s0 + 32 tile * Dout - tpad, a multiple of 4), as a delay-line slot.
-    const int sbm = int((a.s0 + (long) tout0 * Dout - tpad) & (a.pf_cap - 1));
+    const long s0 = a.chunk_ctr ? *a.chunk_ctr * (long) a.nt_chunk : a.s0;
+    const int sbm = int((s0 + (long) tout0 * Dout - tpad) & (a.pf_cap - 1));
     const bool full = (L > 1) || (a.P > 1);
     const int nq0 = (ntw * Dout + tpad) >> 2;   // samples the active lanes read (a partial last tile reads fewer)
 
@@ -1853,7 +1858,8 @@ static void launch_grid_lds_t(const GridLdsArgs &a, cudaStream_t s)
     long nthr = nwin * (1L << (a.rank - 1)) * a.B;
     // Blocks start at a window 0 (a multiple of nwin threads, about 128), so that every other window's
     // predecessor is computed in the same block.
-    int bd = (nwin <= 128) ? int(nwin * (128 / nwin)) : (nwin <= kGridMaxThreads ? int(nwin) : kGridMaxThreads);
+    const int target = (a.block_target > 0) ? std::min(a.block_target, kGridMaxThreads) : 128;
+    int bd = (nwin <= target) ? int(nwin * (target / nwin)) : (nwin <= kGridMaxThreads ? int(nwin) : kGridMaxThreads);
     if (a.q_data) {
         if (a.T % 256) throw std::runtime_error("grid_lds_kernel: int4 input needs a chunk length that is a multiple of 256");
         grid_lds_kernel<Ts, NLEV, true><<<(unsigned) ((nthr + bd - 1) / bd), bd, 0, s>>>(a);
@@ -1991,7 +1997,8 @@ int pf_warp_floats(int Dout, int tpad, int Dcore, int L)
 // The fast kernel needs 4-sample runs of the window (Dout >= 4, tpad and s0 multiples of 4).
 static bool pf_fast_ok(const PfArgs &a)
 {
-    return a.Dout >= 4 && (a.tpad % 4) == 0 && (a.s0 % 4) == 0 && (a.pf_cap % 4) == 0 && a.L <= 5 && a.P <= kPfMaxProfiles;
+    const long s0 = a.chunk_ctr ? (long) a.nt_chunk : a.s0;   // with a counter, s0 is a multiple of nt_chunk
+    return !a.force_general && a.Dout >= 4 && (a.tpad % 4) == 0 && (s0 % 4) == 0 && (a.pf_cap % 4) == 0 && a.L <= 5 && a.P <= kPfMaxProfiles;
 }
 
 template<typename Ts, int L, int DOUT>

@@ -45,6 +45,9 @@ struct Stage1Args
     long s0;                // stream time of the chunk's first sample (ichunk * nt)
     int nt;                 // samples per chunk at this tree's time resolution
     int beam0;              // total-beam index of batch beam 0
+    // If not null, the chunk index is read from device memory at launch (a replayed CUDA graph advances
+    // it): s0 = *chunk_ctr * nt, and in_s0 = *chunk_ctr * nt for delay-line inputs (in_mask != -1).
+    const long *chunk_ctr;
 };
 
 // Stage 2 (one output tree): stage-1 delay lines -> two-phase subband tree -> peak-finder delay lines.
@@ -75,6 +78,7 @@ struct Stage2Args
     long s0;
     int nt;
     int beam0;
+    const long *chunk_ctr;  // if not null: s0 = *chunk_ctr * nt
 };
 
 // Arguments of the peak-finding kernel (one output tree).
@@ -91,6 +95,9 @@ struct PfArgs
     int Dout, Dcore, tpad;
     long s0;                // stream time of the chunk's first sample
     int beam0;
+    const long *chunk_ctr;  // if not null: s0 = *chunk_ctr * nt_chunk
+    int nt_chunk;
+    int force_general;      // 1: the general kernel even where the fast one applies
 };
 
 // Arguments of the fused tree-gridding + lagged-downsampling kernel.
@@ -113,6 +120,8 @@ struct GridLdsArgs
     // bytes, two samples per byte (low nibble first); q_scoff (B, F, T/256, 2) fp16 (scale, offset).
     const void *q_data;
     const void *q_scoff;
+    const long *chunk_ctr;  // if not null: the chunk index is *chunk_ctr instead of ichunk
+    int block_target;       // threads per block to aim for (0: 128); blocks hold whole rows of windows
 };
 
 // Floats of persistent state per block of the stage kernels (host and device agree by construction).

@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(kPatchW * 32) patch_kernel(PatchArgs a)
     const int m = (tok >> 16) & 0xffff, p = (tok >> 8) & 0xff, tf = tok & 0xff;
     const int l = p ? (p - 1) / 3 : 0;
     const int dt = min(t.Dcore, 1 << l);
-    const long s0 = a.ichunk * t.nt_ds;
+    const long s0 = (a.chunk_ctr ? *a.chunk_ctr : a.ichunk) * t.nt_ds;
     // Last sample of the winning trial (the decode_argmax convention), placed at window time 23,
     // shifted so that the window ends inside the chunk.
     const long tend = s0 + (long) a.itime[b] * t.Dout + tf + dt - 1;

@@ -49,6 +49,7 @@ struct PatchArgs
     const uint32_t *token;
     float threshold;
     long ichunk;
+    const long *chunk_ctr;  // if not null: the chunk index is *chunk_ctr instead of ichunk
     int beam0, B;
     uint16_t *patches;    // (B, 1728) fp16 bits, layout ((d * 32 + j) * 6 + w)
     int *valid;           // (B,) 1 where peak >= threshold

@@ -154,7 +154,8 @@ class CandidateGenerator:
                 channels with 10-sigma sinusoids) or weaker versions whose dedispersed SNR overlaps
                 the pulses'.
     The event's candidate is the stronger of its two chunks' per-beam peaks (6 sigma threshold); its
-    label is 1 for pulses. Inputs are float16 N(0, 1) samples written into the dedisperser's input
+    label is 1 for pulses. The dedisperser's state is cleared before every event, so that no event sees
+    an earlier one through the delay lines. Inputs are float16 N(0, 1) samples written into the dedisperser's input
     slot on the GPU; peak-finding weights are pirate's analytic ones for unit variance.
     """
 
@@ -273,6 +274,9 @@ class CandidateGenerator:
                 elif k == 2:
                     ev.update(strong=bool(self.rng.random() < 0.3))
                 events.append(ev)
+            # A fresh history for every event pair: no event sees an earlier event's pulse or RFI through
+            # the delay lines (the downsampled trees' lags reach tens of chunks back).
+            self.dd.zero_state()
             r0 = self._run_chunk(events, 0)
             r1 = self._run_chunk(events, 1)
             for b, ev in enumerate(events):
