@@ -181,6 +181,10 @@ int pb2_dd_create(const pb2_plan *plan, const pb2_dd_params *params, pb2_dedispe
 int pb2_dd_allocate(pb2_dedisperser *dd);
 /* Device bytes held by the dedisperser after allocate(). */
 int pb2_dd_device_bytes(const pb2_dedisperser *dd, long *nbytes);
+/* Pinned host bytes of the stage-1 delay lines spilled to host memory: rows whose stage-2 readers are
+ * more than the config's max_gpu_clag chunks behind (pirate's MegaRingbuf host zones,
+ * src_lib/MegaRingbuf.cpp:155-183); 0 when nothing is spilled (max_gpu_clag 10000, the default). */
+int pb2_dd_host_bytes(const pb2_dedisperser *dd, long *nbytes);
 /* GpuDedisperser::acquire_input, src_lib/GpuDedisperser.cpp:796; shape3 = (beams_per_batch, nfreq, nt_in) */
 int pb2_dd_acquire_input(pb2_dedisperser *dd, long seq_id, void *stream, void **ptr, long *shape3);
 /* int4 input, the raw format GpuDedisperser::time dequantizes into the input before dedispersing

@@ -90,6 +90,7 @@ def lib():
         "pb2_dd_create": (ctypes.c_int, [vp, ctypes.POINTER(_DdParams), ctypes.POINTER(vp)]),
         "pb2_dd_allocate": (ctypes.c_int, [vp]),
         "pb2_dd_device_bytes": (ctypes.c_int, [vp, lp]),
+        "pb2_dd_host_bytes": (ctypes.c_int, [vp, lp]),
         "pb2_dd_acquire_input": (ctypes.c_int, [vp, ctypes.c_long, vp, ctypes.POINTER(vp), lp]),
         "pb2_dd_release_input": (ctypes.c_int, [vp, ctypes.c_long, vp]),
         "pb2_dd_acquire_input_int4": (ctypes.c_int, [vp, ctypes.c_long, vp, ctypes.POINTER(vp), ctypes.POINTER(vp), lp]),
@@ -438,6 +439,12 @@ class GpuDedisperser:
     def device_bytes(self):
         n = ctypes.c_long()
         _check(lib().pb2_dd_device_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def host_bytes(self):
+        """Pinned host bytes of the delay lines spilled beyond the config's max_gpu_clag."""
+        n = ctypes.c_long()
+        _check(lib().pb2_dd_host_bytes(self._h, ctypes.byref(n)))
         return n.value
 
     def kernels_per_batch(self):

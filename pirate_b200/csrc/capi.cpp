@@ -423,6 +423,11 @@ int pb2_dd_device_bytes(const pb2_dedisperser *dd, long *nbytes)
     return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(nbytes); *nbytes = long(dd->d->device_bytes()); });
 }
 
+int pb2_dd_host_bytes(const pb2_dedisperser *dd, long *nbytes)
+{
+    return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(nbytes); *nbytes = long(dd->d->host_bytes()); });
+}
+
 int pb2_dd_acquire_input(pb2_dedisperser *dd, long seq_id, void *stream, void **ptr, long *shape3)
 {
     return guard([&] {

@@ -4,6 +4,8 @@
 #include "avar.hpp"
 
 #include <algorithm>
+#include <limits>
+#include <map>
 #include <chrono>
 #include <cstring>
 #include <sstream>
@@ -67,6 +69,7 @@ GpuDedisperser::~GpuDedisperser()
     cudaGetDevice(&dev);
     cudaSetDevice(params.cuda_device_id);
     if (compute) cudaStreamSynchronize(compute);
+    for (Stage1 &st : s1) if (st.host) cudaFreeHost(st.host);
     for (auto &v : tev) for (auto &pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     auto kill = [](vector<cudaEvent_t> &v) { for (cudaEvent_t e : v) if (e) cudaEventDestroy(e); v.clear(); };
@@ -115,7 +118,9 @@ int GpuDedisperser::kernels_per_batch() const
 {
     // candidate stage: beam peaks, patches, then the MLP (3 GEMMs) and the score mask, or the mask alone
     const int cand = sift ? (2 + (sifter ? 4 : 1)) : 0;
-    return 1 + int(plan.num_primary_trees) + stage2_launches() + int(plan.ntrees) + cand;
+    int spill = 0;
+    for (const Stage1 &st : s1) spill += st.nspill ? 2 : 0;
+    return 1 + int(plan.num_primary_trees) + spill + stage2_launches() + int(plan.ntrees) + cand;
 }
 
 void GpuDedisperser::enable_sifter(float threshold, Sifter *sf)
@@ -285,6 +290,7 @@ void GpuDedisperser::allocate()
         const long rank = plan.config.toplevel_tree_rank, nt = plan.nt_in, F = plan.nfreq, N = pow2(rank);
         const long npri = plan.num_primary_trees;
         total_bytes = 0;
+        host_total = 0;
         auto add = [&](DeviceBuffer &d, size_t n) { d.alloc(n); total_bytes += n; };
 
         // Tree gridding table (src_lib/TreeGriddingKernel.cu:80-97): channel n covers input channels
@@ -330,25 +336,100 @@ void GpuDedisperser::allocate()
             add(st.state, size_t(total_beams) * st.nblocks * st.state_per_block * sizeof(float));
 
             long nrows = pow2(R1 + A1);
-            vector<long> off(nrows);
-            vector<int> cap(nrows);
-            long tot = 0;
-            for (long row = 0; row < nrows; row++) {
-                // one sample more than the lags need: stage 2 also reads the sample before its first
-                cap[row] = int(round_up(plan.max_row_lag[p][row] + st.nt + 1, 32));
-                off[row] = tot;
-                tot += cap[row];
+            // Chunk offsets d = ceil((lag + 1) / nt) of every row's readers (this primary tree's stage-2
+            // trees). A row whose readers all have the same d >= 2, above the config's max_gpu_clag, is
+            // spilled to host memory (MegaRingbuf's host zones, src_lib/MegaRingbuf.cpp:155-183).
+            vector<long> dlo(nrows, std::numeric_limits<long>::max()), dhi(nrows, -1);
+            for (const DedispersionTree &t : plan.trees) {
+                if (t.primary_tree_index != p) continue;
+                for (long a = 0; a < pow2(t.dd_rank); a++)
+                    for (long d = 0; d < pow2(t.amb_rank); d++) {
+                        long row = a * pow2(t.amb_rank) + d;
+                        long dc = (rb_lag(a, d, t.amb_rank, t.dd_rank, p > 0) + st.nt) / st.nt;   // ceil((lag + 1) / nt)
+                        dlo[row] = std::min(dlo[row], dc);
+                        dhi[row] = std::max(dhi[row], dc);
+                    }
             }
+            vector<char> spill(nrows, 0);
+            for (long row = 0; row < nrows; row++)
+                spill[row] = (dhi[row] >= 2 && dlo[row] == dhi[row] && dlo[row] > plan.config.max_gpu_clag);
+
+            // Per beam: block by block, the block's resident lines then its spilled rows' write slots
+            // (nt samples); then every spilled row's read ring (2 nt samples).
+            vector<long> off(nrows), off_r(nrows);
+            vector<int> cap(nrows), cap_r(nrows);
+            long tot = 0;
+            for (long blk = 0; blk < st.nblocks; blk++) {
+                for (long r = 0; r < pow2(R1); r++) {
+                    long row = blk * pow2(R1) + r;
+                    if (spill[row]) continue;
+                    // one sample more than the lags need: stage 2 also reads the sample before its first
+                    cap[row] = cap_r[row] = int(round_up(plan.max_row_lag[p][row] + st.nt + 1, 32));
+                    off[row] = off_r[row] = tot;
+                    tot += cap[row];
+                }
+                for (long r = 0; r < pow2(R1); r++) {
+                    long row = blk * pow2(R1) + r;
+                    if (!spill[row]) continue;
+                    cap[row] = st.nt;
+                    off[row] = tot;
+                    tot += st.nt;
+                }
+            }
+            std::map<long, std::vector<long>> zones;   // d -> spilled rows
+            for (long row = 0; row < nrows; row++)
+                if (spill[row]) {
+                    cap_r[row] = 2 * st.nt;
+                    off_r[row] = tot;
+                    tot += 2 * st.nt;
+                    zones[dlo[row]].push_back(row);
+                }
             st.ring_beam_stride = tot;
             // The stage-1 kernel indexes a block's 2^R1 delay lines with 32-bit offsets.
             for (long blk = 0; blk < st.nblocks; blk++) {
-                long end = (blk + 1 < st.nblocks) ? off[(blk + 1) * pow2(R1)] : tot;
-                if (end - off[blk * pow2(R1)] >= (1L << 31))
+                long lo = std::numeric_limits<long>::max(), hi = 0;
+                for (long r = 0; r < pow2(R1); r++) {
+                    long row = blk * pow2(R1) + r;
+                    lo = std::min(lo, off[row]);
+                    hi = std::max(hi, off[row] + cap[row]);
+                }
+                if (hi - lo >= (1L << 31) || off[blk * pow2(R1)] != lo)
                     throw runtime_error("GpuDedisperser::allocate(): stage-1 delay lines of one block exceed 2^31 samples");
             }
             st.ring_off.upload(off.data(), off.size() * sizeof(long));
             st.ring_cap.upload(cap.data(), cap.size() * sizeof(int));
+            st.ring_off_r.upload(off_r.data(), off_r.size() * sizeof(long));
+            st.ring_cap_r.upload(cap_r.data(), cap_r.size() * sizeof(int));
             add(st.ring, size_t(total_beams) * tot * esize);
+
+            // Host zones: zone d holds S = d + 1 chunk slots of its rows for every beam.
+            vector<SpillRow> srows;
+            long hb = 0;
+            for (auto &z : zones) {
+                const long d = z.first, nz = long(z.second.size());
+                for (long k = 0; k < nz; k++) {
+                    long row = z.second[k];
+                    SpillRow sr;
+                    sr.w_off = off[row];
+                    sr.r_off = off_r[row];
+                    sr.h_base = hb;
+                    sr.n_z = int(nz);
+                    sr.k = int(k);
+                    sr.S = int(d + 1);
+                    sr.d = int(d);
+                    srows.push_back(sr);
+                }
+                hb += (d + 1) * total_beams * nz * st.nt;
+            }
+            st.nspill = int(srows.size());
+            if (st.nspill) {
+                st.spill_rows.upload(srows.data(), srows.size() * sizeof(SpillRow));
+                st.host_bytes = size_t(hb) * esize;
+                CUDA_CHECK(cudaHostAlloc(&st.host, st.host_bytes, cudaHostAllocMapped | cudaHostAllocPortable));
+                memset(st.host, 0, st.host_bytes);
+                CUDA_CHECK(cudaHostGetDevicePointer(&st.host_dev, st.host, 0));
+                host_total += st.host_bytes;
+            }
 
             if (p > 0) {
                 st.lds_cap = next_pow2(st.nt + (1L << R1) - 1);
@@ -592,6 +673,26 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         a.chunk_ctr = ctr;
         cudaEvent_t t2 = tk ? tick(2, nullptr) : nullptr;
         launch_stage1(a, dtype_code, st.nblocks, int(B), s);
+        if (st.nspill) {
+            // host spill: this chunk of the spilled rows to their host zones, and the chunk that
+            // stage 2 reads next from the host into the read rings
+            SpillArgs sa;
+            memset(&sa, 0, sizeof(sa));
+            sa.ring = st.ring.ptr;
+            sa.ring_beam_stride = st.ring_beam_stride;
+            sa.host = st.host_dev;
+            sa.rows = st.spill_rows.as<SpillRow>();
+            sa.nrows = st.nspill;
+            sa.nt = st.nt;
+            sa.esize = int(esize);
+            sa.total_beams = int(total_beams);
+            sa.beam0 = beam0;
+            sa.B = int(B);
+            sa.ichunk = ichunk;
+            sa.chunk_ctr = ctr;
+            launch_spill_g2h(sa, s);
+            launch_spill_h2g(sa, s);
+        }
         if (tk) tick(2, t2);
     }
 
@@ -607,8 +708,8 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         a.state_per_block = st.state_per_block;
         a.state = st.state.as<float>();
         a.ring = src.ring.ptr;
-        a.ring_off = src.ring_off.as<long>();
-        a.ring_cap = src.ring_cap.as<int>();
+        a.ring_off = src.ring_off_r.as<long>();   // spilled rows are read from their read rings
+        a.ring_cap = src.ring_cap_r.as<int>();
         a.ring_beam_stride = src.ring_beam_stride;
         a.amb_rank = t.amb_rank;
         a.uflag = (t.primary_tree_index > 0) ? 1 : 0;

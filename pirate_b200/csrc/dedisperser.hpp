@@ -127,6 +127,9 @@ public:
 
     // Device bytes held by allocate() (for reporting).
     size_t device_bytes() const { return total_bytes; }
+    // Pinned host bytes of the spilled delay lines (rows whose readers are more than the config's
+    // max_gpu_clag chunks behind).
+    size_t host_bytes() const { return host_total; }
     // Number of kernels launched per (chunk, batch).
     int kernels_per_batch() const;
     int stage2_launches() const;
@@ -164,6 +167,7 @@ private:
     int dtype_code = 0;
     size_t esize = 4;
     size_t total_bytes = 0;
+    size_t host_total = 0;
     cudaStream_t compute = nullptr;
 
     // Per-slot events.
@@ -178,6 +182,12 @@ private:
     struct Stage1
     {
         DeviceBuffer ring, ring_off, ring_cap, state;
+        // stage-2 read tables (the same as ring_off/ring_cap except for spilled rows: their read rings),
+        // the spilled-row table, and the rows' host zones (mapped pinned memory)
+        DeviceBuffer ring_off_r, ring_cap_r, spill_rows;
+        void *host = nullptr, *host_dev = nullptr;
+        size_t host_bytes = 0;
+        int nspill = 0;
         long ring_beam_stride = 0, state_per_block = 0;
         int nblocks = 0, nt = 0, rank = 0;
         long lds_cap = 0;

@@ -419,6 +419,46 @@ void launch_pulse_inject(void *out, int dtype, long nfreq, long nt, long row_str
     check_launch("pulse_inject_kernel");
 }
 
+// ---------------------------------------------------------------------------------------------
+// Host spill copies (see SpillArgs): one warp per (beam, spilled row), 16-byte vectors (a chunk row is
+// nt * esize bytes, a multiple of 64; every offset is a multiple of 32 samples).
+
+__device__ __forceinline__ long spill_mod(long x, long m) { long r = x % m; return r < 0 ? r + m : r; }
+
+template<bool G2H>
+__global__ void __launch_bounds__(256) spill_kernel(SpillArgs a)
+{
+    const long w = (long) blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= (long) a.nrows * a.B) return;
+    const int j = int(w % a.nrows), b = int(w / a.nrows), bt = a.beam0 + b;
+    const SpillRow r = a.rows[j];
+    const long c = a.chunk_ctr ? *a.chunk_ctr : a.ichunk;
+    const long q = G2H ? c : c - r.d + 1;   // chunk moved this step
+    const long slot = spill_mod(q, r.S);
+    char *dev = (char *) a.ring + ((long) bt * a.ring_beam_stride + (G2H ? r.w_off : r.r_off + spill_mod(q, 2) * a.nt)) * a.esize;
+    char *host = (char *) a.host + (r.h_base + ((slot * a.total_beams + bt) * r.n_z + r.k) * (long) a.nt) * a.esize;
+    const int nv = a.nt * a.esize / 16;
+    const uint4 *src = (const uint4 *) (G2H ? dev : host);
+    uint4 *dst = (uint4 *) (G2H ? host : dev);
+    for (int i = lane; i < nv; i += 32) dst[i] = src[i];
+}
+
+static void launch_spill(const SpillArgs &a, bool g2h, cudaStream_t s)
+{
+    if (a.nrows <= 0 || a.B <= 0) return;
+    if (!a.ring || !a.host || !a.rows) throw std::runtime_error("spill: null pointer");
+    if ((a.nt * a.esize) % 64) throw std::runtime_error("spill: chunk rows must be a multiple of 64 bytes");
+    const long warps = (long) a.nrows * a.B;
+    const unsigned grid = (unsigned) ((warps + 7) / 8);
+    if (g2h) spill_kernel<true><<<grid, 256, 0, s>>>(a);
+    else spill_kernel<false><<<grid, 256, 0, s>>>(a);
+    check_launch("spill_kernel");
+}
+
+void launch_spill_g2h(const SpillArgs &a, cudaStream_t s) { launch_spill(a, true, s); }
+void launch_spill_h2g(const SpillArgs &a, cudaStream_t s) { launch_spill(a, false, s); }
+
 constexpr int kGridMaxThreads = 512;
 
 template<typename Ts, int NLEV, bool Q>

@@ -154,6 +154,34 @@ void launch_beam_peaks(const BeamPeakArgs &a, int dtype, long nbeams, cudaStream
 void launch_pulse_inject(void *out, int dtype, long nfreq, long nt, long row_stride, long chunk_it0, const long *it0,
                          const long *cnt, const long *off, const float *data, float weight, cudaStream_t s);
 
+// Host spill of stage-1 delay lines (the MegaRingbuf host zones of pirate, src_lib/MegaRingbuf.cpp:155-183,
+// and its g2h/h2g copies, src_lib/GpuDedisperser.cpp:628-707). A spilled row's readers all need chunks
+// d = ceil((lag + 1) / nt) >= 2 back; on the GPU it keeps a one-chunk write slot (stage 1 writes chunk c
+// there) and a two-chunk read ring (stage 2 reads chunks c - d and c - d + 1 there); in mapped pinned host
+// memory its zone (all rows of equal d) keeps S = d + 1 chunk slots per beam. Per step, after stage 1,
+// the g2h kernel copies every spilled row's chunk c to host slot c mod S, and the h2g kernel copies chunk
+// c - d + 1 from host slot (c - d + 1) mod S into read-ring half (c - d + 1) mod 2.
+struct SpillRow
+{
+    long w_off;     // write slot (nt samples) in the beam's delay-line region
+    long r_off;     // read ring (2 nt samples) in the beam's delay-line region
+    long h_base;    // the row's zone in the host buffer: element (slot, beam, k, t) at
+                    // h_base + ((slot * total_beams + beam) * n_z + k) * nt + t
+    int n_z, k, S, d;
+};
+struct SpillArgs
+{
+    void *ring;                 // stage-1 delay lines (total_beams regions of ring_beam_stride samples)
+    long ring_beam_stride;
+    void *host;                 // mapped pinned host buffer (device-accessible pointer)
+    const SpillRow *rows;       // device table of the spilled rows
+    int nrows, nt, esize, total_beams, beam0, B;
+    long ichunk;
+    const long *chunk_ctr;      // if not null: the chunk index is *chunk_ctr
+};
+void launch_spill_g2h(const SpillArgs &a, cudaStream_t s);
+void launch_spill_h2g(const SpillArgs &a, cudaStream_t s);
+
 void launch_grid_lds(const GridLdsArgs &a, int dtype, cudaStream_t s);
 // int4 -> out_dtype dequantization of (nbeams, nfreq, ntime) samples (ntime a multiple of 256).
 void launch_dequantize(void *out, int out_dtype, const void *data, const void *scales_offsets, long nbeams, long nfreq,

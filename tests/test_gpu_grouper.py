@@ -83,7 +83,8 @@ def test_toy_grouper_on_dedisperser_outputs(pb2lib):
     from pirate_b200.grouper import ToyGrouper, make_events
     cfg = H.toy_config(rank=8, nfreq=300, nt=512, dtype="float16", beams_per_gpu=4, beams_per_batch=2)
     plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(cfg))
-    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=2)
+    # both batches of a chunk are launched before they are consumed: two output slots
+    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=2, nbatches_out=2)
     dd.allocate()
     dd.fill_analytic_weights(np.ones(plan.nfreq))
     grouper = ToyGrouper(dd, plan, consumer_id=0, snr_threshold=3.5)
