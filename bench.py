@@ -28,6 +28,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -275,6 +277,149 @@ def run_ours(args, rank, world):
                 bytes_per_beam=per_beam)
 
 
+def cfg3_groups(scale):
+    """BASELINE config 3's mix: tree ranks 12, 14, 16 in proportions 1:1:2 (64 beams at scale 1),
+    downsampling depths (primary trees) 3, 4, 5 spread over each rank's beams, 2048-sample chunks,
+    float16 storage; channels = 2^rank / 4 (the benchmark's 16384 channels for rank 16)."""
+    out = []
+    for rank, nbeams in ((12, 16), (14, 16), (16, 32)):
+        n = max(3, int(round(nbeams * scale)))
+        split = [n - 2 * (n // 3), n // 3, n // 3]
+        for depth, k in zip((3, 4, 5), split):
+            if k:
+                out.append((rank, depth, k))
+    return out
+
+
+def group_config(rank, depth, beams, dtype="float16", max_gpu_clag=10000):
+    prim = [dict(num_early_triggers=0, max_width=32, dm_downsampling=0, time_downsampling=0,
+                 wt_dm_downsampling=2 ** ((rank - (1 if i else 0)) // 2), wt_time_downsampling=64) for i in range(depth)]
+    return dict(zone_nfreq=[2 ** rank // 4], zone_freq_edges=[400.0, 800.0], time_sample_ms=SAMPLE_MS,
+                toplevel_tree_rank=rank, time_samples_per_chunk=CHUNK, dtype=dtype,
+                frequency_subband_counts=[0, 0, 0, 0, 1], primary_trees=prim, beams_per_gpu=beams,
+                beams_per_batch=beams, num_active_batches=1, future_write_max_samples=0, max_gpu_clag=max_gpu_clag)
+
+
+def run_batched(scale, steps, reps=3):
+    """BASELINE config 3 (uneven beams, one replayed CUDA graph per chunk, autotuned schedule): returns
+    the real-time beams, ms per step and the record. Inputs are N(0,1) float16 noise resident in every
+    group's input slot."""
+    import torch
+    import pirate_b200 as pb
+    groups = cfg3_groups(scale)
+    plans = [pb.DedispersionPlan(pb.DedispersionConfig.from_dict(group_config(r, d, b))) for r, d, b in groups]
+    bd = pb.BatchedDedisperser(plans, cuda_device_id=int(os.environ.get("LOCAL_RANK", "0")))
+    bd.allocate()
+    for g, p in enumerate(plans):
+        bd.fill_analytic_weights(g, np.ones(p.nfreq))
+        bd.input(g).normal_()
+    torch.cuda.synchronize()
+    rec = bd.autotune(reps=reps)
+    for g in range(len(plans)):
+        bd.input(g).normal_()
+    torch.cuda.synchronize()
+    for _ in range(3):
+        bd.step()
+    ms = bd.time_steps(steps)
+    nbeams = sum(b for _, _, b in groups)
+    res = dict(value=round(nbeams * CHUNK_SECONDS / (ms * 1e-3), 2), unit="beams", ms_per_step=round(ms, 4), beams=nbeams,
+               groups=[dict(rank=r, primary_trees=d, beams=b) for r, d, b in groups],
+               device_bytes=bd.device_bytes(), kernels_per_step=bd.kernels_per_step(),
+               autotune=dict(chosen=rec["chosen"], candidates=len(rec["candidates"])))
+    del bd
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_spill(steps, beams=8, clag=2):
+    """The benchmark plan with delay lines more than 'clag' chunks deep in pinned host memory (g2h/h2g
+    copy kernels every chunk): real-time beams, device and host bytes."""
+    import torch
+    import pirate_b200 as pb
+    cfg = bench_config(beams, "float16")
+    cfg["max_gpu_clag"] = clag
+    plan = pb.DedispersionPlan(pb.DedispersionConfig.from_dict(cfg))
+    dd = pb.GpuDedisperser(plan, cuda_device_id=int(os.environ.get("LOCAL_RANK", "0")), num_consumers=1)
+    dd.allocate()
+    dd.fill_analytic_weights(np.ones(plan.nfreq))
+    stream = torch.cuda.current_stream()
+    seq = [0]
+
+    def step():
+        s = seq[0]
+        a = dd.acquire_input(s, stream)
+        if s == 0:
+            a.normal_()
+        dd.release_input_and_launch_dd_kernels(s, stream)
+        dd.acquire_output(0, s, stream)
+        dd.release_output(0, s, stream)
+        seq[0] += 1
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    res = dict(value=round(beams * CHUNK_SECONDS / (ms * 1e-3), 2), unit="beams", ms_per_step=round(ms, 4), beams=beams,
+               max_gpu_clag=clag, device_bytes=dd.device_bytes(), host_bytes=dd.host_bytes(),
+               device_bytes_per_beam=round(dd.device_bytes() / beams / 1e9, 3))
+    del dd
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_sifter(steps, beams=8, n_train=6144, n_test=3072):
+    """The learned candidate sifter: trained by its own kernels on candidates of the small pipeline
+    (rank 12, 5 primary trees; sifter_study.config('small')), recall at false-alarm fractions of the
+    held-out negatives against the plain threshold; then the candidate stage (per-beam peaks, patches,
+    MLP) attached to the benchmark workload, its device time per step (CUDA events)."""
+    import torch
+    import pirate_b200 as pb
+    from pirate_b200 import sifter_study as SS
+    res, sf = SS.study(SS.config("small"), n_train, n_test, epochs=40, fars=(1e-2, 1e-3))
+    cfg = bench_config(beams, "float16")
+    plan = pb.DedispersionPlan(pb.DedispersionConfig.from_dict(cfg))
+    dd = pb.GpuDedisperser(plan, cuda_device_id=int(os.environ.get("LOCAL_RANK", "0")), num_consumers=1)
+    dd.allocate()
+    dd.fill_analytic_weights(np.ones(plan.nfreq))
+    dd.enable_sifter(6.0, sf)
+    stream = torch.cuda.current_stream()
+    seq = [0]
+
+    def step():
+        s = seq[0]
+        a = dd.acquire_input(s, stream)
+        if s == 0:
+            a.normal_()
+        dd.release_input_and_launch_dd_kernels(s, stream)
+        dd.acquire_output(0, s, stream)
+        dd.release_output(0, s, stream)
+        seq[0] += 1
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    dd.enable_timing(True)
+    for _ in range(steps):
+        step()
+    kt = dd.kernel_times()
+    dd.enable_timing(False)
+    tot = sum(v[0] for v in kt.values())
+    out = dict(recall=res["recall"], test_positives=res["test_positives"], test_negatives=res["test_negatives"],
+               train_candidates=res["train_valid"], workload="rank 12 from 2048 channels, 5 primary trees, 1024-sample chunks, "
+               "float16; pulses (simpulse model), noise and RFI events",
+               candidate_stage_ms_per_step=round(kt["sifter"][0] / steps, 4),
+               candidate_stage_share=round(kt["sifter"][0] / tot, 4) if tot else None,
+               candidate_stage_config="benchmark workload, %d beams: per-beam peaks, 9x32x6 patches, MLP on the tensor cores" % beams)
+    del dd, sf
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_plain_fp32(args, steps):
     """The plain fp32 GPU path (BASELINE config 2's shape): one beam, float32 storage, float32 N(0,1)
     input resident in the input slot (no int4 input, no batching), same plan otherwise. Returns
@@ -405,6 +550,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--beams", type=int, default=8)
     ap.add_argument("--no-plain-fp32", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the config-3 batched leg")
+    ap.add_argument("--no-spill", action="store_true", help="skip the host-spill leg")
+    ap.add_argument("--no-sifter", action="store_true", help="skip the learned-sifter leg")
+    ap.add_argument("--batched-scale", type=float, default=0.5, help="config 3's beam counts x this")
     ap.add_argument("--dtype", default="float16", choices=["float16", "bfloat16", "float32"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -521,14 +670,26 @@ def main():
         line["capacity_beams"] = r["capacity_beams"]
         line["capacity_note"] = ("beams whose lag state and buffers fit in this GPU's HBM (%.2f GB per beam); "
                                  "the real-time figure above is throughput" % (r["bytes_per_beam"] / 1e9))
-    if world == 1 and not args.no_plain_fp32:
-        del r["dd"]
+    if world == 1:
+        # free the headline run's device memory before the other legs
         import gc
+        import torch
+        r.pop("dd", None)
         gc.collect()
+        torch.cuda.empty_cache()
+    if world == 1 and not args.no_plain_fp32:
         pv, pms = run_plain_fp32(args, max(10, min(args.steps, 30)))
         line["plain_fp32"] = {"value": round(pv, 2), "unit": "beams", "ms_per_step": round(pms, 4),
                               "config": "1 beam, float32 storage, float32 input resident on the device, no batching"}
         line["vs_plain_fp32"] = round(value / pv, 3)
+    if world == 1 and not args.no_batched:
+        line["batched_cfg3"] = run_batched(args.batched_scale, max(10, min(args.steps, 30)))
+        line["batched_cfg3"]["note"] = ("config 3's mix at %g x its 64 beams: the full 64 need about 300 GB of lag "
+                                        "state (fp16), more than this GPU's HBM plus host memory" % args.batched_scale)
+    if world == 1 and not args.no_spill:
+        line["spill"] = run_spill(max(5, min(args.steps, 10)))
+    if world == 1 and not args.no_sifter:
+        line["sifter"] = run_sifter(max(5, min(args.steps, 20)))
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             kind = cpu_kind()
