@@ -1584,7 +1584,9 @@ __host__ __device__ constexpr int pf_tpad_of(int L) { return (2 << L) > 4 ? (2 <
 // The kernel body. g holds the per-level constants (a compile-time constant object when DOUT > 0, so
 // the unrolled level loop sees them as immediates); gr is the same geometry passed at launch, used
 // where the level is only known at run time.
-template<typename Ts, int L, int DOUT>
+// CTR: the chunk index comes from the device counter (replayed CUDA graphs). It is a template flag
+// because reading it costs the kernel about 26 registers, which the direct launches should not pay.
+template<typename Ts, int L, int DOUT, bool CTR>
 __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, const PfGeom &gr)
 {
     extern __shared__ float sm[];
@@ -1614,7 +1616,8 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
     const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
     const int mask = int(a.pf_cap - 1);
     // Window sample 0 (stream time s0 + 32 tile * Dout - tpad, a multiple of 4), as a delay-line slot.
-    const long s0 = a.chunk_ctr ? *a.chunk_ctr * (long) a.nt_chunk : a.s0;
+    long s0 = a.s0;
+    if constexpr (CTR) s0 = *a.chunk_ctr * (long) a.nt_chunk;
     const int sbm = int((s0 + (long) tout0 * Dout - tpad) & (a.pf_cap - 1));
     const bool full = (L > 1) || (a.P > 1);
     const int nq0 = (ntw * Dout + tpad) >> 2;   // samples the active lanes read (a partial last tile reads fewer)
@@ -1873,14 +1876,14 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
 
 // DOUT > 0: compiled for that output time downsampling (with Dcore = min(DOUT, 8) and the plan's tpad
 // for L levels); DOUT = 0: any Dout >= 4, geometry read from the launch arguments.
-template<typename Ts, int L, int DOUT>
+template<typename Ts, int L, int DOUT, bool CTR>
 __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom gr)
 {
     if constexpr (DOUT > 0) {
         constexpr PfGeom gc = pf_geom(DOUT, pf_dcore_of(DOUT), pf_tpad_of(L), L, sizeof(Ts));
-        pf_fast_body<Ts, L, DOUT>(a, gc, gr);
+        pf_fast_body<Ts, L, DOUT, CTR>(a, gc, gr);
     } else {
-        pf_fast_body<Ts, L, 0>(a, gr, gr);
+        pf_fast_body<Ts, L, 0, CTR>(a, gr, gr);
     }
 }
 
@@ -2045,9 +2048,14 @@ template<typename Ts, int L, int DOUT>
 static void launch_pf_fast(const PfArgs &a, const PfGeom &g, int B, cudaStream_t s)
 {
     size_t sm = (size_t) kPfWarps * g.warp_floats * sizeof(float);
-    set_smem(pf_fast_kernel<Ts, L, DOUT>, sm);
     dim3 grid((a.nt_out + 31) / 32, (a.ndm_out + kPfWarps - 1) / kPfWarps, B);
-    pf_fast_kernel<Ts, L, DOUT><<<grid, kPfWarps * 32, sm, s>>>(a, g);
+    if (a.chunk_ctr) {
+        set_smem(pf_fast_kernel<Ts, L, DOUT, true>, sm);
+        pf_fast_kernel<Ts, L, DOUT, true><<<grid, kPfWarps * 32, sm, s>>>(a, g);
+    } else {
+        set_smem(pf_fast_kernel<Ts, L, DOUT, false>, sm);
+        pf_fast_kernel<Ts, L, DOUT, false><<<grid, kPfWarps * 32, sm, s>>>(a, g);
+    }
     check_launch("pf_fast_kernel");
 }
 
