@@ -1,4 +1,5 @@
-"""Builds the B200 dedispersion library in-tree: pirate_b200/libpirate_b200.so (sm_100a).
+"""Builds the B200 dedispersion library in-tree: pirate_b200/libpirate_b200.so (sm_100a), and the
+pybind11 module pirate_b200/_pirate_b200_pybind*.so over it (pirate's pybind11 class surface).
 
 Usage: python -m pirate_b200.build [--force] [--verbose]
 """
@@ -26,6 +27,27 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
 
 def _newest(paths):
     return max(os.path.getmtime(p) for p in paths)
+
+
+def build_pybind(force=False):
+    """The pybind11 module (pirate_b200/csrc/pybind.cpp over include/pirate_b200.hpp), linked to the
+    library with an $ORIGIN rpath."""
+    import sysconfig
+    import pybind11
+    out = os.path.join(HERE, "_pirate_b200_pybind" + sysconfig.get_config_var("EXT_SUFFIX"))
+    root = os.path.dirname(HERE)
+    deps = [os.path.join(CSRC, "pybind.cpp"), os.path.join(root, "include", "pirate_b200.hpp"),
+            os.path.join(root, "include", "pirate_b200.h"), LIB]
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= _newest(deps):
+        return out
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-shared", "-fPIC", "-std=c++17",
+           "-I" + sysconfig.get_paths()["include"], "-I" + pybind11.get_include(),
+           os.path.join(CSRC, "pybind.cpp"), "-o", out + ".tmp", "-L" + HERE, "-lpirate_b200", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("pybind11 module build failed:\n%s\n%s" % (r.stdout, r.stderr))
+    os.replace(out + ".tmp", out)
+    return out
 
 
 def build(force=False, verbose=False):
@@ -60,4 +82,5 @@ def build(force=False, verbose=False):
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
+    build_pybind(force="--force" in sys.argv)
     print(LIB)
