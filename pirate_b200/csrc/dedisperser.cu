@@ -117,7 +117,7 @@ void GpuDedisperser::stop(std::exception_ptr e)
 int GpuDedisperser::kernels_per_batch() const
 {
     // candidate stage: beam peaks, patches, then the MLP (3 GEMMs) and the score mask, or the mask alone
-    const int cand = sift ? (2 + (sifter ? 4 : 1)) : 0;
+    const int cand = sift ? (3 + (sifter ? 4 : 1)) : 0;
     int spill = 0;
     for (const Stage1 &st : s1) spill += st.nspill ? 2 : 0;
     return 1 + int(plan.num_primary_trees) + spill + stage2_launches() + int(plan.ntrees) + cand;
@@ -135,6 +135,9 @@ void GpuDedisperser::enable_sifter(float threshold, Sifter *sf)
         if (!d_cand.ptr) {
             d_cand.alloc(size_t(nbatches_out) * 8 * B * 4);
             d_patches.alloc(size_t(nbatches_out) * B * kPatchLen * sizeof(uint16_t));
+            // split beam-peak reduction: about four waves of blocks over the (tree, beam) pairs
+            peak_split = int(std::max(1L, std::min(256L, (4L * 148 + plan.ntrees * B - 1) / (plan.ntrees * B))));
+            d_peak_scratch.alloc(size_t(B) * plan.ntrees * peak_split * 16);
         }
         memset(&patch_args, 0, sizeof(patch_args));
         patch_args.ntrees = int(plan.ntrees);
@@ -786,7 +789,7 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         ba.idm = (int *) (cb + 2 * B);
         ba.itime = (int *) (cb + 3 * B);
         ba.token = (uint32_t *) (cb + 4 * B);
-        launch_beam_peaks(ba, dtype_code, B, s);
+        launch_beam_peaks_split(ba, dtype_code, B, d_peak_scratch.ptr, peak_split, s);
         PatchArgs pa = patch_args;
         for (long i = 0; i < plan.ntrees; i++) {
             const DedispersionTree &t = plan.trees[i];

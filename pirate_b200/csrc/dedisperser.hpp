@@ -217,7 +217,8 @@ private:
     bool sift = false;
     float sift_threshold = 0.0f;
     Sifter *sifter = nullptr;
-    DeviceBuffer d_cand, d_patches;
+    DeviceBuffer d_cand, d_patches, d_peak_scratch;
+    int peak_split = 1;
     PatchArgs patch_args;
     void *acquire_slot(long seq_id, cudaStream_t stream, void **int4);
 };

@@ -368,6 +368,131 @@ __global__ void __launch_bounds__(1024) beam_peak_kernel(BeamPeakArgs a)
     }
 }
 
+struct PeakPartial
+{
+    float v;      // maximum of the slice (-inf if empty)
+    int nan;      // the slice holds a NaN
+    long i;       // first position of the maximum in the tree (kNone if none)
+};
+
+// Grid (nsplit, ntrees, nbeams): block (s, t, b) reduces slice s of tree t of beam b.
+template<typename T>
+__global__ void __launch_bounds__(256) beam_peak_split_kernel(BeamPeakArgs a, PeakPartial *part, int nsplit)
+{
+    constexpr int V = PeakVec<T>::N;
+    constexpr long kNone = 0x7fffffffffffffffL;
+    __shared__ float rv[8];
+    __shared__ long ri[8];
+    __shared__ int rn[8];
+    const int s = blockIdx.x, t = blockIdx.y, b = blockIdx.z;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long n = a.ndm[t] * a.nt[t];
+    const T *x = (const T *) a.out_max[t] + (long) b * n;
+    float bv = -INFINITY;
+    long bi = kNone;
+    bool nan = false;
+    if (n % V == 0 && ((uintptr_t) x & 15) == 0) {
+        const long nv = n / V, per = (nv + nsplit - 1) / nsplit;
+        const long lo = (long) s * per, hi = min(nv, lo + per);
+        const uint4 *xv = (const uint4 *) x;
+        for (long j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+            const uint4 q = __ldg(xv + j);
+#pragma unroll
+            for (int k = 0; k < V; k++) {
+                const float v = PeakVec<T>::get(q, k);
+                nan |= (v != v);
+                if (v > bv) { bv = v; bi = j * V + k; }
+            }
+        }
+    } else {
+        const long per = (n + nsplit - 1) / nsplit;
+        const long lo = (long) s * per, hi = min(n, lo + per);
+        for (long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            const float v = to_f(x[i]);
+            nan |= (v != v);
+            if (v > bv) { bv = v; bi = i; }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        peak_take(__shfl_down_sync(0xffffffffu, bv, o), __shfl_down_sync(0xffffffffu, bi, o), bv, bi);
+    const bool wnan = __any_sync(0xffffffffu, nan);
+    if (lane == 0) { rv[warp] = bv; ri[warp] = bi; rn[warp] = wnan; }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        bv = (lane < nw) ? rv[lane] : -INFINITY;
+        bi = (lane < nw) ? ri[lane] : kNone;
+        const bool tn = __any_sync(0xffffffffu, (lane < nw) && rn[lane]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            peak_take(__shfl_down_sync(0xffffffffu, bv, o), __shfl_down_sync(0xffffffffu, bi, o), bv, bi);
+        if (lane == 0) {
+            PeakPartial &p = part[((long) b * a.ntrees + t) * nsplit + s];
+            p.v = bv;
+            p.nan = tn ? 1 : 0;
+            p.i = bi;
+        }
+    }
+}
+
+// One warp per beam: per tree (in order) the slices' maximum with the first position, a tree holding a
+// NaN passed over, then the first tree with the strictly largest maximum (beam_peak_kernel's rules).
+__global__ void beam_peak_final_kernel(BeamPeakArgs a, const PeakPartial *part, int nsplit)
+{
+    constexpr long kNone = 0x7fffffffffffffffL;
+    const int b = blockIdx.x, lane = threadIdx.x;
+    float gv = -INFINITY;
+    int gt = -1;
+    long gi = 0;
+    for (int t = 0; t < a.ntrees; t++) {
+        float bv = -INFINITY;
+        long bi = kNone;
+        bool nan = false;
+        for (int s = lane; s < nsplit; s += 32) {
+            const PeakPartial p = part[((long) b * a.ntrees + t) * nsplit + s];
+            nan |= (p.nan != 0);
+            peak_take(p.v, p.i, bv, bi);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            peak_take(__shfl_down_sync(0xffffffffu, bv, o), __shfl_down_sync(0xffffffffu, bi, o), bv, bi);
+        const bool tnan = __any_sync(0xffffffffu, nan);
+        if (lane == 0 && !tnan && bv > gv) { gv = bv; gt = t; gi = bi; }
+    }
+    if (lane == 0) {
+        a.peak[b] = gv;
+        a.tree[b] = gt;
+        if (gt >= 0) {
+            const long nt = a.nt[gt];
+            a.idm[b] = int(gi / nt);
+            a.itime[b] = int(gi % nt);
+            a.token[b] = a.out_argmax[gt][(long) b * a.ndm[gt] * nt + gi];
+        } else {
+            a.idm[b] = -1;
+            a.itime[b] = -1;
+            a.token[b] = 0;
+        }
+    }
+}
+
+void launch_beam_peaks_split(const BeamPeakArgs &a, int dtype, long nbeams, void *scratch, int nsplit, cudaStream_t s)
+{
+    if (a.ntrees <= 0 || a.ntrees > kBeamPeakMaxTrees) throw std::runtime_error("beam_peaks: bad number of trees");
+    if (!scratch || nsplit < 1 || nsplit > 1024) throw std::runtime_error("beam_peaks: bad split scratch");
+    if (nbeams <= 0) return;
+    if (nbeams > 65535) throw std::runtime_error("beam_peaks: too many beams for the split reduction");
+    dim3 grid((unsigned) nsplit, (unsigned) a.ntrees, (unsigned) nbeams);
+    PeakPartial *part = (PeakPartial *) scratch;
+    if (dtype == 0) beam_peak_split_kernel<float><<<grid, 256, 0, s>>>(a, part, nsplit);
+    else if (dtype == 1) beam_peak_split_kernel<__half><<<grid, 256, 0, s>>>(a, part, nsplit);
+    else if (dtype == 2) beam_peak_split_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(a, part, nsplit);
+    else throw std::runtime_error("beam_peaks: bad dtype");
+    check_launch("beam_peak_split_kernel");
+    beam_peak_final_kernel<<<(unsigned) nbeams, 32, 0, s>>>(a, part, nsplit);
+    check_launch("beam_peak_final_kernel");
+}
+
 void launch_beam_peaks(const BeamPeakArgs &a, int dtype, long nbeams, cudaStream_t s)
 {
     if (a.ntrees < 0 || a.ntrees > kBeamPeakMaxTrees) throw std::runtime_error("beam_peaks: bad number of trees");

@@ -146,6 +146,9 @@ struct BeamPeakArgs
     uint32_t *token;
 };
 void launch_beam_peaks(const BeamPeakArgs &a, int dtype, long nbeams, cudaStream_t s);
+// The same reduction spread over nsplit blocks per (tree, beam) (a few beams fill a few SMs otherwise),
+// then one warp per beam combines the partial results. scratch: nbeams * ntrees * nsplit * 16 bytes.
+void launch_beam_peaks_split(const BeamPeakArgs &a, int dtype, long nbeams, void *scratch, int nsplit, cudaStream_t s);
 
 // Adds a sparse pulse (channel f: cnt[f] samples from sample index it0[f], values data[off[f] ...])
 // times 'weight' to the chunk out (nfreq rows of row_stride elements, dtype 0/1/2 = f32/f16/bf16)

@@ -107,3 +107,29 @@ def test_toy_grouper_on_dedisperser_outputs(pb2lib):
         assert np.array_equal(peak, ref[0])
         want = make_events(plan, ichunk, *ref, 3.5)
         assert np.array_equal(events, want)
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float16"])
+def test_candidate_stage_peaks(pb2lib, dtype):
+    """The candidate stage's split per-beam reduction (many blocks per tree and beam, then one warp per
+    beam) gives the numpy loop's peaks on real outputs, NaN inputs included."""
+    import torch
+    cfg = H.toy_config(rank=9, nfreq=300, nt=512, dtype=dtype, beams_per_gpu=6, beams_per_batch=6)
+    plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(cfg))
+    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=1)
+    dd.allocate()
+    dd.fill_analytic_weights(np.ones(plan.nfreq))
+    dd.enable_sifter(threshold=4.0)
+    xs = H.make_inputs(cfg, 4, seed=44)
+    xs[2][3, :, 10:20] = np.nan      # beam 3 of chunk 2: NaN in every channel
+    for x in xs:
+        with dd.get_input() as a:
+            a.copy_(torch.from_numpy(x).to(a.dtype).to(a.device))
+        with dd.get_output(0, sync=True) as out:
+            want = toy_peaks_numpy([m.float().cpu().numpy() for m in out.out_max],
+                                   [a.cpu().numpy().view(np.uint32) for a in out.out_argmax])
+            c = out.candidates
+            got = (c["peak"], c["tree"], c["idm"], c["itime"], c["token"])
+            _check(got, want)
+            valid = c["valid"].cpu().numpy()
+            assert np.array_equal(valid == 1, want[0] >= 4.0)
