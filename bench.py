@@ -40,13 +40,14 @@ METRIC = "real-time beams/B200 (rank 16, fp16)"
 L2_BYTES = 126 * 2 ** 20
 
 
-def bench_config(beams, dtype, rank=16, npri=5, nfreq=16384):
+def bench_config(beams, dtype, rank=16, npri=5, nfreq=16384, streams=1):
+    """streams > 1: the beams form that many batches, one per compute stream (num_active_batches)."""
     prim = [dict(num_early_triggers=0, max_width=32, dm_downsampling=0, time_downsampling=0,
                  wt_dm_downsampling=64, wt_time_downsampling=64) for _ in range(npri)]
     return dict(zone_nfreq=[nfreq], zone_freq_edges=[400.0, 800.0], time_sample_ms=SAMPLE_MS,
                 toplevel_tree_rank=rank, time_samples_per_chunk=CHUNK, dtype=dtype,
                 frequency_subband_counts=[0, 0, 0, 0, 1], primary_trees=prim,
-                beams_per_gpu=beams, beams_per_batch=beams, num_active_batches=1,
+                beams_per_gpu=beams, beams_per_batch=beams // streams, num_active_batches=streams,
                 future_write_max_samples=0, max_gpu_clag=10000)
 
 
@@ -139,9 +140,10 @@ def run_ours(args, rank, world):
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    cfg = bench_config(args.beams, args.dtype, args.rank, args.npri, args.nfreq)
+    cfg = bench_config(args.beams, args.dtype, args.rank, args.npri, args.nfreq, args.streams)
     plan = pb.DedispersionPlan(pb.DedispersionConfig.from_dict(cfg))
     dd = pb.GpuDedisperser(plan, cuda_device_id=dev, num_consumers=1)
+    nbat = args.streams   # batches per chunk
     dd.allocate()
     tdt = getattr(torch, args.dtype)
 
@@ -178,16 +180,18 @@ def run_ours(args, rank, world):
     dq_data, dq_so = quantized_input("cuda")
 
     def step_device():
-        """One chunk of all beams; the int4 input stays resident in the (single) input slot."""
-        s = seq[0]
-        d, so = dd.acquire_input_int4(s, stream)
-        if s == 0:
-            d.copy_(dq_data)
-            so.copy_(dq_so)
-        dd.release_input_and_launch_dd_kernels(s, stream)
-        dd.acquire_output(0, s, stream)
-        dd.release_output(0, s, stream)
-        seq[0] += 1
+        """One chunk of all beams (nbat batches); the int4 input stays resident in the input slots."""
+        s0 = seq[0]
+        for s in range(s0, s0 + nbat):
+            d, so = dd.acquire_input_int4(s, stream)
+            if s < nbat:
+                d.copy_(dq_data)
+                so.copy_(dq_so)
+            dd.release_input_and_launch_dd_kernels(s, stream)
+        for s in range(s0, s0 + nbat):
+            dd.acquire_output(0, s, stream)
+            dd.release_output(0, s, stream)
+        seq[0] += nbat
 
     for _ in range(args.warmup):
         step_device()
@@ -225,30 +229,33 @@ def run_ours(args, rank, world):
     out_stream = torch.cuda.Stream()
     torch.cuda.synchronize()
     outs_host = None
-    h2d = h_data.numel() + h_so.numel() * 2
+    h2d = (h_data.numel() + h_so.numel() * 2) * nbat
     d2h = 0
     esize = torch.tensor([], dtype=tdt).element_size()
     for t in plan.trees:
-        d2h += plan.beams_per_batch * t.ndm_out * t.nt_out * (esize + 4)
+        d2h += args.beams * t.ndm_out * t.nt_out * (esize + 4)
 
     def step_e2e():
         nonlocal outs_host
-        s = seq[0]
-        d, so = dd.acquire_input_int4(s, copy_stream)
-        with torch.cuda.stream(copy_stream):
-            d.copy_(h_data, non_blocking=True)
-            so.copy_(h_so, non_blocking=True)
-        dd.release_input_and_launch_dd_kernels(s, copy_stream)
-        o = dd.acquire_output(0, s, out_stream)
-        if outs_host is None:
-            outs_host = [(torch.empty(m.shape, dtype=m.dtype, pin_memory=True),
-                          torch.empty(a.shape, dtype=a.dtype, pin_memory=True)) for m, a in zip(o.out_max, o.out_argmax)]
-        with torch.cuda.stream(out_stream):
-            for (hm, ha), m, a in zip(outs_host, o.out_max, o.out_argmax):
-                hm.copy_(m, non_blocking=True)
-                ha.copy_(a, non_blocking=True)
-        dd.release_output(0, s, out_stream)
-        seq[0] += 1
+        s0 = seq[0]
+        for s in range(s0, s0 + nbat):
+            d, so = dd.acquire_input_int4(s, copy_stream)
+            with torch.cuda.stream(copy_stream):
+                d.copy_(h_data, non_blocking=True)
+                so.copy_(h_so, non_blocking=True)
+            dd.release_input_and_launch_dd_kernels(s, copy_stream)
+        for s in range(s0, s0 + nbat):
+            o = dd.acquire_output(0, s, out_stream)
+            if outs_host is None:
+                outs_host = [[(torch.empty(m.shape, dtype=m.dtype, pin_memory=True),
+                               torch.empty(a.shape, dtype=a.dtype, pin_memory=True)) for m, a in zip(o.out_max, o.out_argmax)]
+                             for _ in range(nbat)]
+            with torch.cuda.stream(out_stream):
+                for (hm, ha), m, a in zip(outs_host[s - s0], o.out_max, o.out_argmax):
+                    hm.copy_(m, non_blocking=True)
+                    ha.copy_(a, non_blocking=True)
+            dd.release_output(0, s, out_stream)
+        seq[0] += nbat
 
     e2e_steps = max(4, min(args.steps, 32))
     for _ in range(3):
@@ -268,12 +275,12 @@ def run_ours(args, rank, world):
     per_beam = dd.device_bytes() / float(args.beams)
     capacity_beams = int(torch.cuda.get_device_properties(dev).total_memory // per_beam)
 
-    alg = dd.algorithmic_bytes()
+    alg = [x * nbat for x in dd.algorithmic_bytes()]   # per step: every batch of the chunk
     # The gridding class reads int4 data and scales/offsets instead of storage-dtype samples.
-    alg[0] += float(plan.beams_per_batch) * plan.nfreq * (plan.nt_in / 2 + plan.nt_in / 256 * 4 - plan.nt_in * esize)
+    alg[0] += float(args.beams) * plan.nfreq * (plan.nt_in / 2 + plan.nt_in / 256 * 4 - plan.nt_in * esize)
     return dict(plan=plan, dd=dd, ms_per_step=ms_per_step, e2e_ms_per_step=ems / e2e_steps, ktimes=ktimes,
                 alg=alg, clocks=clk.summary(), h2d=h2d, d2h=d2h, device_bytes=dd.device_bytes(),
-                kernels_per_batch=dd.kernels_per_batch(), capacity_beams=capacity_beams,
+                kernels_per_batch=dd.kernels_per_batch() * nbat, capacity_beams=capacity_beams,
                 bytes_per_beam=per_beam)
 
 
@@ -549,7 +556,9 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--beams", type=int, default=8)
+    ap.add_argument("--streams", type=int, default=1, help="compute streams (num_active_batches); beams split into that many batches")
     ap.add_argument("--no-plain-fp32", action="store_true")
+    ap.add_argument("--no-streams-leg", action="store_true", help="skip the two-compute-stream leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the config-3 batched leg")
     ap.add_argument("--no-spill", action="store_true", help="skip the host-spill leg")
     ap.add_argument("--no-sifter", action="store_true", help="skip the learned-sifter leg")
@@ -564,6 +573,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.streams < 1 or args.beams % args.streams:
+        sys.exit("bench.py: --beams must be a multiple of --streams")
 
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         # One process per GPU: relaunch under torchrun (rendezvous on 127.0.0.1).
@@ -580,7 +591,8 @@ def main():
         sys.exit("bench.py: --gpus %d but WORLD_SIZE=%d" % (args.gpus, world))
     cfg_json = {"workload": "rank-16 tree, 16384 channels 400-800 MHz, 5 primary trees (time downsampling 1-16), "
                             "2048-sample chunks, widths to 32 per tree, full-band search",
-                "beams_per_gpu": args.beams, "chunk_samples": CHUNK, "sample_ms": SAMPLE_MS,
+                "beams_per_gpu": args.beams, "beams_per_batch": args.beams // args.streams,
+                "compute_streams": args.streams, "chunk_samples": CHUNK, "sample_ms": SAMPLE_MS,
                 "storage": args.dtype, "parallelism": "replicas x%d (beams shard, no collective)" % args.gpus,
                 "l2": "inputs and lag state exceed L2 (126 MB) every step",
                 "input": "int4 samples + fp16 (scale, offset) per 256 samples (pirate's raw format), "
@@ -677,6 +689,21 @@ def main():
         r.pop("dd", None)
         gc.collect()
         torch.cuda.empty_cache()
+    if world == 1 and args.streams == 1 and args.beams % 2 == 0 and not args.no_streams_leg:
+        # The same workload as two batches of beams on two compute streams (num_active_batches 2): the
+        # batches' kernels overlap, filling each other's partial waves. Reported beside the headline,
+        # whose per-kernel event timing needs one stream.
+        import copy
+        a2 = copy.copy(args)
+        a2.streams, a2.steps = 2, max(10, min(args.steps, 30))
+        r2 = run_ours(a2, rank, world)
+        r2.pop("dd", None)
+        gc.collect()
+        torch.cuda.empty_cache()
+        line["two_streams"] = {"value": round(real_time_beams(args.beams, world, r2["ms_per_step"] * 1e-3, CHUNK_SECONDS), 2),
+                               "e2e": round(real_time_beams(args.beams, world, r2["e2e_ms_per_step"] * 1e-3, CHUNK_SECONDS), 2),
+                               "ms_per_step": round(r2["ms_per_step"], 4), "steps": a2.steps,
+                               "config": "%d beams as 2 batches of %d on 2 compute streams" % (args.beams, args.beams // 2)}
     if world == 1 and not args.no_plain_fp32:
         pv, pms = run_plain_fp32(args, max(10, min(args.steps, 30)))
         line["plain_fp32"] = {"value": round(pv, 2), "unit": "beams", "ms_per_step": round(pms, 4),

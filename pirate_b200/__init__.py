@@ -429,6 +429,8 @@ class GpuDedisperser:
         self.nbatches = plan.beams_per_gpu // plan.beams_per_batch
         self.nbatches_out = int(nbatches_out) or plan.num_active_batches
         self.nbatches_wt = int(nbatches_wt) or self.nbatches_out
+        # batch seq_id runs on compute stream seq_id % num_compute_streams (pirate: one stream per active batch)
+        self.num_compute_streams = plan.num_active_batches
         self.dtype = plan.dtype
         self._next_in = 0
         self._next_out = [0] * self.num_consumers

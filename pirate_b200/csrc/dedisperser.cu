@@ -52,6 +52,7 @@ GpuDedisperser::GpuDedisperser(const DedispersionPlan &plan_, const Params &para
     total_beams = plan.beams_per_gpu;
     nbatches = total_beams / B;
     nslots_in = plan.num_active_batches;
+    nstreams = plan.num_active_batches;
     nbatches_out = params.nbatches_out ? params.nbatches_out : plan.num_active_batches;
     nbatches_wt = params.nbatches_wt ? params.nbatches_wt : nbatches_out;
     if (params.num_consumers < 0) throw runtime_error("GpuDedisperser: num_consumers must be >= 0");
@@ -68,7 +69,7 @@ GpuDedisperser::~GpuDedisperser()
     int dev = 0;
     cudaGetDevice(&dev);
     cudaSetDevice(params.cuda_device_id);
-    if (compute) cudaStreamSynchronize(compute);
+    for (cudaStream_t c : computes) cudaStreamSynchronize(c);
     for (Stage1 &st : s1) if (st.host) cudaFreeHost(st.host);
     for (auto &v : tev) for (auto &pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
@@ -77,7 +78,9 @@ GpuDedisperser::~GpuDedisperser()
     kill(ev_in_free);
     kill(ev_out_done);
     for (auto &v : ev_out_released) kill(v);
-    if (compute) cudaStreamDestroy(compute);
+    kill(ev_beams_done);
+    if (ev_sifter) cudaEventDestroy(ev_sifter);
+    for (cudaStream_t c : computes) cudaStreamDestroy(c);
     cudaSetDevice(dev);
 }
 
@@ -106,6 +109,11 @@ auto GpuDedisperser::entry(F &&f) -> decltype(f())
     }
 }
 
+void GpuDedisperser::sync_compute()
+{
+    for (cudaStream_t c : computes) CUDA_CHECK(cudaStreamSynchronize(c));
+}
+
 void GpuDedisperser::stop(std::exception_ptr e)
 {
     std::lock_guard<std::mutex> lk(mtx);
@@ -131,13 +139,13 @@ void GpuDedisperser::enable_sifter(float threshold, Sifter *sf)
         if (sf && (sf->device != params.cuda_device_id || sf->max_batch < B))
             throw runtime_error("GpuDedisperser::enable_sifter(): the sifter must be on this device with max_batch >= beams_per_batch");
         CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
-        CUDA_CHECK(cudaStreamSynchronize(compute));
+        sync_compute();
         if (!d_cand.ptr) {
             d_cand.alloc(size_t(nbatches_out) * 8 * B * 4);
             d_patches.alloc(size_t(nbatches_out) * B * kPatchLen * sizeof(uint16_t));
             // split beam-peak reduction: about four waves of blocks over the (tree, beam) pairs
             peak_split = int(std::max(1L, std::min(256L, (4L * 148 + plan.ntrees * B - 1) / (plan.ntrees * B))));
-            d_peak_scratch.alloc(size_t(B) * plan.ntrees * peak_split * 16);
+            d_peak_scratch.alloc(size_t(nstreams) * B * plan.ntrees * peak_split * 16);
         }
         memset(&patch_args, 0, sizeof(patch_args));
         patch_args.ntrees = int(plan.ntrees);
@@ -233,13 +241,13 @@ void GpuDedisperser::enable_timing(bool on)
 
 // Records an event on the compute stream. With start == nullptr returns a fresh start event;
 // otherwise closes the interval (start, now) for class 'cls'.
-cudaEvent_t GpuDedisperser::tick(int cls, cudaEvent_t start)
+cudaEvent_t GpuDedisperser::tick(int cls, cudaEvent_t start, cudaStream_t s)
 {
     if (!timing) return nullptr;
     cudaEvent_t e;
     if (!ev_pool.empty()) { e = ev_pool.back(); ev_pool.pop_back(); }
     else CUDA_CHECK(cudaEventCreate(&e));
-    CUDA_CHECK(cudaEventRecord(e, compute));
+    CUDA_CHECK(cudaEventRecord(e, s));
     if (start) {
         tev[cls].push_back({start, e});
         if (tev[cls].size() > 256) drain_timing();
@@ -276,7 +284,10 @@ void GpuDedisperser::allocate()
     entry([&]() {
         if (allocated) throw runtime_error("GpuDedisperser::allocate() called twice");
         CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
-        CUDA_CHECK(cudaStreamCreateWithFlags(&compute, cudaStreamNonBlocking));
+        computes.resize(nstreams);
+        for (auto &c : computes) CUDA_CHECK(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
+        compute = computes[0];
+        CUDA_CHECK(cudaEventCreateWithFlags(&ev_sifter, cudaEventDisableTiming));
         auto mk = [](vector<cudaEvent_t> &v, long n) {
             v.resize(n);
             for (auto &e : v) CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -284,6 +295,8 @@ void GpuDedisperser::allocate()
         mk(ev_in_acquired, nslots_in);
         mk(ev_in_free, nslots_in);
         mk(ev_out_done, nbatches_out);
+        mk(ev_beams_done, nbatches);
+        beams_done_recorded.assign(nbatches, false);
         ev_out_released.resize(params.num_consumers);
         for (auto &v : ev_out_released) mk(v, nbatches_out);
         in_free_recorded.assign(nslots_in, false);
@@ -323,7 +336,7 @@ void GpuDedisperser::allocate()
             add(d_qscoff, size_t(nslots_in) * B * F * (nt / 256) * 2 * sizeof(uint16_t));
         }
         slot_int4.assign(nslots_in, false);
-        add(d_tree0, size_t(B) * N * nt * esize);
+        add(d_tree0, size_t(nstreams) * B * N * nt * esize);
         if (npri > 1) add(d_lds_state, size_t(2) * total_beams * (npri - 1) * (N / 2) * sizeof(float));
 
         s1.clear();
@@ -543,7 +556,7 @@ void GpuDedisperser::release_input_and_launch_dd_kernels(long seq_id, cudaStream
         long slot = seq_id % nslots_in;
         CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
         CUDA_CHECK(cudaEventRecord(ev_in_acquired[slot], stream));
-        CUDA_CHECK(cudaStreamWaitEvent(compute, ev_in_acquired[slot], 0));
+        CUDA_CHECK(cudaStreamWaitEvent(computes[seq_id % nstreams], ev_in_acquired[slot], 0));
         launch_batch(seq_id);
         next_rel_in++;
         cv.notify_all();
@@ -552,9 +565,15 @@ void GpuDedisperser::release_input_and_launch_dd_kernels(long seq_id, cudaStream
 
 void GpuDedisperser::launch_batch(long seq_id)
 {
-    const long ichunk = seq_id / nbatches, ibatch = seq_id % nbatches;
-    launch_kernels(ichunk, ibatch, seq_id % nslots_in, seq_id % nbatches_out, seq_id % nbatches_wt, compute, nullptr,
+    const long ichunk = seq_id / nbatches, ibatch = seq_id % nbatches, istream = seq_id % nstreams;
+    cudaStream_t s = computes[istream];
+    // The previous chunk of these beams may have run on another compute stream: its delay lines and
+    // tree state must be complete.
+    if (beams_done_recorded[ibatch]) CUDA_CHECK(cudaStreamWaitEvent(s, ev_beams_done[ibatch], 0));
+    launch_kernels(ichunk, ibatch, seq_id % nslots_in, seq_id % nbatches_out, seq_id % nbatches_wt, s, istream, nullptr,
                    GroupTuning(), true);
+    CUDA_CHECK(cudaEventRecord(ev_beams_done[ibatch], s));
+    beams_done_recorded[ibatch] = true;
 }
 
 void GpuDedisperser::enqueue_chunk(cudaStream_t stream, const long *chunk_ctr, const GroupTuning &tune)
@@ -563,7 +582,7 @@ void GpuDedisperser::enqueue_chunk(cudaStream_t stream, const long *chunk_ctr, c
         if (!allocated) throw runtime_error("GpuDedisperser::enqueue_chunk(): allocate() was not called");
         if (nbatches != 1) throw runtime_error("GpuDedisperser::enqueue_chunk(): needs beams_per_gpu == beams_per_batch");
         if (!chunk_ctr) throw runtime_error("GpuDedisperser::enqueue_chunk(): null chunk counter");
-        launch_kernels(0, 0, 0, 0, 0, stream, chunk_ctr, tune, false);
+        launch_kernels(0, 0, 0, 0, 0, stream, 0, chunk_ctr, tune, false);
     });
 }
 
@@ -595,7 +614,7 @@ void GpuDedisperser::zero_state(cudaStream_t s)
     entry([&]() {
         if (!allocated) throw runtime_error("GpuDedisperser::zero_state(): allocate() was not called");
         CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
-        CUDA_CHECK(cudaStreamSynchronize(compute));   // no batch of this object may still be running
+        sync_compute();   // no batch of this object may still be running
         auto z = [&](const DeviceBuffer &d) { if (d.ptr) CUDA_CHECK(cudaMemsetAsync(d.ptr, 0, d.nbytes, s)); };
         z(d_inputs); z(d_tree0); z(d_lds_state); z(d_qdata); z(d_qscoff); z(d_cand); z(d_patches);
         for (auto &st : s1) { z(st.ring); z(st.state); z(st.lds); }
@@ -604,12 +623,13 @@ void GpuDedisperser::zero_state(cudaStream_t s)
 }
 
 void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long slot_out, long slot_wt, cudaStream_t s,
-                                    const long *ctr, const GroupTuning &tune, bool fences)
+                                    long istream, const long *ctr, const GroupTuning &tune, bool fences)
 {
     const long rank = plan.config.toplevel_tree_rank, nt = plan.nt_in, F = plan.nfreq, N = pow2(rank);
     const long npri = plan.num_primary_trees;
     const int beam0 = int(ibatch * B);
-    const bool tk = (ctr == nullptr);   // kernel timing ticks only on the compute stream
+    const bool tk = (ctr == nullptr);   // kernel timing ticks only on the compute streams
+    char *tree0 = d_tree0.as<char>() + size_t(istream) * B * N * nt * esize;
 
     GridLdsArgs g;
     memset(&g, 0, sizeof(g));
@@ -618,7 +638,7 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         g.q_data = d_qdata.as<char>() + size_t(slot_in) * B * F * (nt / 2);
         g.q_scoff = d_qscoff.as<char>() + size_t(slot_in) * B * F * (nt / 256) * 2 * sizeof(uint16_t);
     }
-    g.tree0 = d_tree0.ptr;
+    g.tree0 = tree0;
     g.chan_f0 = d_grid_f0.as<int>();
     g.chan_cnt = d_grid_cnt.as<int>();
     g.chan_woff = d_grid_woff.as<int>();
@@ -634,9 +654,9 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
     g.chunk_ctr = ctr;
     g.block_target = tune.grid_block;
     g.beam0 = beam0; g.B = int(B); g.total_beams = int(total_beams);
-    cudaEvent_t t0 = tk ? tick(0, nullptr) : nullptr;
+    cudaEvent_t t0 = tk ? tick(0, nullptr, s) : nullptr;
     launch_grid_lds(g, dtype_code, s);
-    if (tk) tick(0, t0);
+    if (tk) tick(0, t0, s);
     if (fences) {
         CUDA_CHECK(cudaEventRecord(ev_in_free[slot_in], s));
         in_free_recorded[slot_in] = true;
@@ -650,7 +670,7 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         a.state_per_block = st.state_per_block;
         a.state = st.state.as<float>();
         if (p == 0) {
-            a.in = d_tree0.ptr;
+            a.in = tree0;
             a.in_beam_stride = N * nt;
             a.in_row_stride = nt;
             a.in_mask = -1;
@@ -674,7 +694,7 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         a.nt = st.nt;
         a.beam0 = beam0;
         a.chunk_ctr = ctr;
-        cudaEvent_t t2 = tk ? tick(2, nullptr) : nullptr;
+        cudaEvent_t t2 = tk ? tick(2, nullptr, s) : nullptr;
         launch_stage1(a, dtype_code, st.nblocks, int(B), s);
         if (st.nspill) {
             // host spill: this chunk of the spilled rows to their host zones, and the chunk that
@@ -696,7 +716,7 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
             launch_spill_g2h(sa, s);
             launch_spill_h2g(sa, s);
         }
-        if (tk) tick(2, t2);
+        if (tk) tick(2, t2, s);
     }
 
     std::vector<Stage2Args> a2(plan.ntrees);
@@ -731,9 +751,9 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
     for (long i0 = 0; i0 < plan.ntrees;) {
         long i1 = i0 + 1;
         while (tune.merge_stage2 && i1 < plan.ntrees && i1 - i0 < kStage2MaxTrees && stage2_same_kernel(a2[i0], a2[i1])) i1++;
-        cudaEvent_t t3 = tk ? tick(3, nullptr) : nullptr;
+        cudaEvent_t t3 = tk ? tick(3, nullptr, s) : nullptr;
         launch_stage2_multi(&a2[i0], &nb2[i0], int(i1 - i0), dtype_code, int(B), s);
-        if (tk) tick(3, t3);
+        if (tk) tick(3, t3, s);
         i0 = i1;
     }
 
@@ -765,13 +785,13 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         a.chunk_ctr = ctr;
         a.nt_chunk = int(t.nt_ds);
         a.force_general = tune.pf_general ? 1 : 0;
-        cudaEvent_t t4 = tk ? tick(4, nullptr) : nullptr;
+        cudaEvent_t t4 = tk ? tick(4, nullptr, s) : nullptr;
         launch_pf(a, dtype_code, int(B), s);
-        if (tk) tick(4, t4);
+        if (tk) tick(4, t4, s);
     }
     if (sift) {
         // Candidate stage: per-beam peak over the trees, patches of the peaks >= threshold, scores.
-        cudaEvent_t t1 = tk ? tick(1, nullptr) : nullptr;
+        cudaEvent_t t1 = tk ? tick(1, nullptr, s) : nullptr;
         float *cb = (float *) d_cand.ptr + size_t(slot_out) * 8 * B;
         BeamPeakArgs ba;
         memset(&ba, 0, sizeof(ba));
@@ -789,7 +809,8 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         ba.idm = (int *) (cb + 2 * B);
         ba.itime = (int *) (cb + 3 * B);
         ba.token = (uint32_t *) (cb + 4 * B);
-        launch_beam_peaks_split(ba, dtype_code, B, d_peak_scratch.ptr, peak_split, s);
+        launch_beam_peaks_split(ba, dtype_code, B, d_peak_scratch.as<char>() + size_t(istream) * B * plan.ntrees * peak_split * 16,
+                                peak_split, s);
         PatchArgs pa = patch_args;
         for (long i = 0; i < plan.ntrees; i++) {
             const DedispersionTree &t = plan.trees[i];
@@ -804,12 +825,16 @@ void GpuDedisperser::launch_kernels(long ichunk, long ibatch, long slot_in, long
         launch_patches(pa, dtype_code, s);
         float *logits = cb + 6 * B, *scores = cb + 7 * B;
         if (sifter) {
+            // one forward pass at a time: the sifter's activations are shared by the compute streams
+            if (sifter_recorded) CUDA_CHECK(cudaStreamWaitEvent(s, ev_sifter, 0));
             sifter->forward(pa.patches, B, logits, s);
+            CUDA_CHECK(cudaEventRecord(ev_sifter, s));
+            sifter_recorded = true;
             launch_mask_scores(logits, pa.valid, scores, int(B), s);
         } else {
             launch_mask_scores(ba.peak, pa.valid, scores, int(B), s);
         }
-        if (tk) tick(1, t1);
+        if (tk) tick(1, t1, s);
     }
     if (fences) {
         CUDA_CHECK(cudaEventRecord(ev_out_done[slot_out], s));
@@ -893,6 +918,7 @@ void GpuDedisperser::fill_all_weights(long itree, const float *host, long nelts)
         if (nelts != expect)
             throw runtime_error("GpuDedisperser::fill_all_weights(): expected " + std::to_string(expect) + " elements "
                                 "(nbatches_wt, beams_per_batch, ndm_wt, nt_wt, nprofiles, N), got " + std::to_string(nelts));
+        sync_compute();   // no launched batch may still read the weights
         CUDA_CHECK(cudaMemcpyAsync(s2[itree].wt.ptr, host, nelts * sizeof(float), cudaMemcpyHostToDevice, compute));
         CUDA_CHECK(cudaStreamSynchronize(compute));
     });
@@ -905,6 +931,7 @@ void GpuDedisperser::fill_analytic_weights(const double *freq_variances, long nf
     entry([&]() {
         if (!allocated) throw runtime_error("GpuDedisperser::fill_analytic_weights(): allocate() was not called");
         std::vector<std::vector<double>> var = pf_analytic_variances(plan, freq_variances, nfreq);
+        sync_compute();   // no launched batch may still read the weights
         for (long itree = 0; itree < plan.ntrees; itree++) {
             std::vector<float> w = pf_weights_from_variances(plan.trees[itree], var[itree]);
             const size_t nb = w.size() * sizeof(float);

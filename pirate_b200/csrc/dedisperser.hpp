@@ -8,7 +8,7 @@
 // Device memory layout (all allocated and zeroed by allocate()):
 //   inputs    nslots_in x (B, nfreq, nt_in)                     storage dtype
 //   int4 in   nslots_in x (B, nfreq, nt_in/2) bytes + (B, nfreq, nt_in/256, 2) fp16 scales/offsets
-//   tree0     (B, 2^rank, nt_in) level-0 tree                    storage dtype
+//   tree0     nstreams x (B, 2^rank, nt_in) level-0 tree         storage dtype
 //   lds[p]    (total_beams, 2^(rank-1), cap_p) delay lines       storage dtype, cap_p = 2^k >= nt_p + 2^s1dd - 1
 //   ring[p]   per stage-1 output row (a, dm_brev): a delay line of capacity max_lag(row) + nt_p (rounded to 32)
 //   pfring[i] (total_beams, ndm_out, M, cap_i) subband rows       storage dtype, cap_i = 2^k >= nt + tpad + Dout
@@ -147,13 +147,15 @@ public:
     const DedispersionPlan plan;
     const Params params;
     long nbatches = 0, B = 0, total_beams = 0, nslots_in = 0, nbatches_out = 0, nbatches_wt = 0;
+    long num_compute_streams() const { return nstreams; }
 
 private:
     void check_alive() const;
     template<typename F> auto entry(F &&f) -> decltype(f());
     void launch_batch(long seq_id);
     void launch_kernels(long ichunk, long ibatch, long slot_in, long slot_out, long slot_wt, cudaStream_t s,
-                        const long *chunk_ctr, const GroupTuning &tune, bool fences);
+                        long istream, const long *chunk_ctr, const GroupTuning &tune, bool fences);
+    void sync_compute();
 
     std::mutex mtx;
     std::condition_variable cv;                     // signalled by release_output() and stop()
@@ -168,7 +170,18 @@ private:
     size_t esize = 4;
     size_t total_bytes = 0;
     size_t host_total = 0;
-    cudaStream_t compute = nullptr;
+    // Compute streams, one per active batch (pirate's CudaStreamPool compute streams,
+    // include/pirate/CudaStreamPool.hpp:27-39): batch seq_id runs on computes[seq_id % nstreams] with
+    // its own level-0 tree and reduction scratch; batches of the same beams are ordered by
+    // ev_beams_done[ibatch] (pirate's cdd2 event-ring wait on seq_id - nbatches,
+    // src_lib/GpuDedisperser.cpp:1008-1011), and the sifter's forward passes by ev_sifter.
+    std::vector<cudaStream_t> computes;
+    cudaStream_t compute = nullptr;   // computes[0]: weight uploads and clears, after sync_compute()
+    long nstreams = 1;
+    std::vector<cudaEvent_t> ev_beams_done;
+    std::vector<bool> beams_done_recorded;
+    cudaEvent_t ev_sifter = nullptr;
+    bool sifter_recorded = false;
 
     // Per-slot events.
     std::vector<cudaEvent_t> ev_in_acquired, ev_in_free, ev_out_done;
@@ -205,7 +218,7 @@ private:
     double tms[5] = {0, 0, 0, 0, 0};
     long tcount[5] = {0, 0, 0, 0, 0};
     std::vector<cudaEvent_t> ev_pool;
-    cudaEvent_t tick(int cls, cudaEvent_t start);
+    cudaEvent_t tick(int cls, cudaEvent_t start, cudaStream_t s);
     void drain_timing();
 
     std::vector<Stage1> s1;

@@ -197,3 +197,40 @@ def test_two_batches_two_consumers(pb2lib):
             dd.release_output(1, held[1].pop(0))
     while held[1]:
         dd.release_output(1, held[1].pop(0))
+
+
+def test_batches_overlap_on_two_compute_streams(pb2lib):
+    """Three beam batches per chunk on two compute streams (num_active_batches 2), every batch of a chunk
+    launched before any output is read, so consecutive chunks of one batch alternate streams and the
+    batches of a chunk overlap on the GPU. Outputs equal the fp32 oracle bit for bit, and each beam's
+    candidate peak (per-stream reduction scratch) is its largest output over the trees."""
+    import torch
+    cfg, plan, dd = _small(pb2lib, beams_per_gpu=6, beams_per_batch=2, num_active_batches=2, synchronous=False,
+                           nbatches_out=6, release_timeout_ms=20000)
+    assert dd.num_compute_streams == 2
+    orc, ws = _weights(cfg, 5, dd.nbatches_wt)
+    for i, w in enumerate(ws):
+        dd.fill_all_weights(i, w)
+    dd.enable_sifter(threshold=1e30)
+    nchunks, nb = 3, 3
+    xs = H.make_inputs(cfg, nchunks, seed=10)
+    _, ores = H.run_oracle(cfg, xs, ws, 1, 32)
+    for ichunk in range(nchunks):
+        seqs = range(ichunk * nb, (ichunk + 1) * nb)
+        for seq in seqs:
+            _launch(dd, seq, xs[seq])
+        for seq in seqs:
+            out = dd.acquire_output(0, seq, sync=True)
+            assert out.ibeam == (seq % nb) * 2 and out.ichunk_zero_based == ichunk
+            best = np.full(2, -np.inf)
+            for i in range(orc.ntrees):
+                m = out.out_max[i].float().cpu().numpy().astype(np.float64)
+                a = out.out_argmax[i].cpu().numpy().view(np.uint32)
+                assert np.array_equal(m, ores[seq][0][i]), (seq, i)
+                assert np.array_equal(a, ores[seq][1][i]), (seq, i)
+                best = np.maximum(best, m.reshape(2, -1).max(axis=1))
+            peak = out.candidates["peak"].cpu().numpy().astype(np.float64)
+            assert np.array_equal(peak, best), seq
+            assert not out.candidates["valid"].cpu().numpy().any()
+            dd.release_output(0, seq)
+    torch.cuda.synchronize()
