@@ -112,3 +112,29 @@ def test_int4_fp32_vs_oracle(pb2lib):
         for i in range(orc.ntrees):
             assert np.array_equal(g[seq][0][i], ores[seq][0][i]), "seq %d tree %d out_max" % (seq, i)
             assert np.array_equal(g[seq][1][i], ores[seq][1][i]), "seq %d tree %d out_argmax" % (seq, i)
+
+
+@pytest.mark.parametrize("nfreq,npri", [(300, 5), (900, 5), (2000, 2)])
+def test_int4_lookup_tables_vs_oracle(pb2lib, nfreq, npri):
+    """The gridding kernel's per-warp int4 lookup tables: 16-sample windows (5 primary trees: two scale
+    blocks per warp), channel pairs whose input rows exceed the tables mixed with pairs that fit
+    (900 channels), and pairs that never fit (2000). float32 is bitwise the oracle; float16 equals the
+    separate dequantization kernel followed by the dedisperser."""
+    prim = H._prim(8, [(0, 16, 0)] + [(0, 8, 0)] * (npri - 1), wt_time=16)
+    for dtype in ("float32", "float16"):
+        cfg = H.toy_config(rank=8, nfreq=nfreq, nt=1024, dtype=dtype, subbands=[2, 2, 1], beams_per_gpu=2,
+                           beams_per_batch=1, primary_trees=prim)
+        qs = _quantized_chunks(cfg, 2, seed=nfreq)
+        orc, _ = H.run_oracle(cfg, [], [])
+        ws = H.make_weights(orc, seed=11)
+        g = _run_int4(pb2lib, cfg, qs, ws, fused=True)
+        if dtype == "float32":
+            B, F, T = cfg["beams_per_batch"], sum(cfg["zone_nfreq"]), cfg["time_samples_per_chunk"]
+            xs = [O.dequantize(d, s, B, F, T) for d, s in qs]
+            _, want = H.run_oracle(cfg, xs, ws, 1, 32)
+        else:
+            want = _run_int4(pb2lib, cfg, qs, ws, fused=False)
+        for seq in range(len(qs)):
+            for i in range(orc.ntrees):
+                assert np.array_equal(g[seq][0][i], want[seq][0][i]), (dtype, seq, i)
+                assert np.array_equal(g[seq][1][i], want[seq][1][i]), (dtype, seq, i)
