@@ -232,25 +232,40 @@ __device__ __forceinline__ void lut_build(const GridLdsArgs &a, int b, int rlo, 
     __syncwarp();
 }
 
-// grid_run<Ts, W, true> through the warp's tables (W a multiple of 8, t0 in scale block blk0 + myblk).
+// The nibble words of a window of W samples (W / 8 words) of input row 'row' (t0 a multiple of 8).
+template<int W>
+__device__ __forceinline__ void lut_words(const GridLdsArgs &a, long row, long t0, uint32_t (&q)[W / 8])
+{
+    const uint32_t *p = (const uint32_t *) ((const uint8_t *) a.q_data + row * (a.T >> 1) + (t0 >> 1));
+#pragma unroll
+    for (int v = 0; v < W / 8; v++) q[v] = p[v];
+}
+
+// o += w * (row's samples), the samples looked up in table L.
+template<int W>
+__device__ __forceinline__ void lut_accum(float (&o)[W], float w, const uint32_t (&q)[W / 8], const float *L)
+{
+#pragma unroll
+    for (int v = 0; v < W / 8; v++)
+#pragma unroll
+        for (int k8 = 0; k8 < 8; k8++) o[8 * v + k8] = __fadd_rn(o[8 * v + k8], __fmul_rn(w, L[(q[v] >> (4 * k8)) & 15]));
+}
+
+// grid_run<Ts, W, true> of tree channel n through the warp's tables (W a multiple of 8, t0 in scale
+// block blk0 + myblk), summed in ascending input channel. q0 holds the words of the channel's first
+// input row (loaded by the caller before the tables were built); later rows are loaded here.
 template<typename Ts, int W, int NBLK>
-__device__ __forceinline__ void grid_run_lut(const GridLdsArgs &a, int b, long n, long t0, float (&o)[W], const float *lut,
-                                             int rlo, int myblk)
+__device__ __forceinline__ void grid_run_lut(const GridLdsArgs &a, int b, int f0, int cnt, int woff, long t0, float (&o)[W],
+                                             const uint32_t (&q0)[W / 8], const float *lut, int rlo, int myblk)
 {
 #pragma unroll
     for (int i = 0; i < W; i++) o[i] = 0.0f;
-    const int f0 = a.chan_f0[n], cnt = a.chan_cnt[n], woff = a.chan_woff[n];
-    for (int k = 0; k < cnt; k++) {
-        const float w = a.chan_w[woff + k];
-        const long row = (long) b * a.F + f0 + k;
-        const float *L = lut + ((f0 + k - rlo) * NBLK + myblk) * 16;
-        const uint32_t *q = (const uint32_t *) ((const uint8_t *) a.q_data + row * (a.T >> 1) + (t0 >> 1));
-#pragma unroll
-        for (int v = 0; v < W / 8; v++) {
-            const uint32_t word = q[v];
-#pragma unroll
-            for (int k8 = 0; k8 < 8; k8++) o[8 * v + k8] = __fadd_rn(o[8 * v + k8], __fmul_rn(w, L[(word >> (4 * k8)) & 15]));
-        }
+    if (cnt > 0)
+        lut_accum<W>(o, a.chan_w[woff], q0, lut + ((f0 - rlo) * NBLK + myblk) * 16);
+    for (int k = 1; k < cnt; k++) {
+        uint32_t q[W / 8];
+        lut_words<W>(a, (long) b * a.F + f0 + k, t0, q);
+        lut_accum<W>(o, a.chan_w[woff + k], q, lut + ((f0 + k - rlo) * NBLK + myblk) * 16);
     }
 }
 
@@ -666,13 +681,19 @@ __global__ void __launch_bounds__(kGridMaxThreads) grid_lds_kernel(GridLdsArgs a
             const int rhi = max(fa + ca, fb + cb);
             use_lut = (rhi - rlo) <= kLutRows;
             if (use_lut) {
+                // The first input row of each channel is loaded before the tables are built, so that its
+                // latency overlaps that of the (scale, offset) loads.
+                uint32_t qa[W0 / 8], qb[W0 / 8];
+                lut_words<W0>(a, (long) b * a.F + (ca ? fa : rlo), t0, qa);
+                lut_words<W0>(a, (long) b * a.F + (cb ? fb : rlo), t0, qb);
+                const int wa = a.chan_woff[2 * c], wb = a.chan_woff[2 * c + 1];
                 const int lane = threadIdx.x & 31;
                 const long blk0 = ((long) (win - lane) * W0) >> 8;
                 float *lut = lut_sh + (threadIdx.x >> 5) * (kLutRows * NBLK * 16);
                 lut_build<Ts, NBLK>(a, b, rlo, rhi - rlo, blk0, lut, lane);
                 const int myblk = int((t0 >> 8) - blk0);
-                grid_run_lut<Ts, W0, NBLK>(a, b, 2 * c, t0, r0, lut, rlo, myblk);
-                grid_run_lut<Ts, W0, NBLK>(a, b, 2 * c + 1, t0, r1, lut, rlo, myblk);
+                grid_run_lut<Ts, W0, NBLK>(a, b, fa, ca, wa, t0, r0, qa, lut, rlo, myblk);
+                grid_run_lut<Ts, W0, NBLK>(a, b, fb, cb, wb, t0, r1, qb, lut, rlo, myblk);
             }
         }
     }
