@@ -812,6 +812,40 @@ __device__ __forceinline__ void bfly_l0_shared(float &v0, float &v1, float *h, i
     if (lane == 31) *h = x;
 }
 
+// Two butterflies of the same lag L at once: pair A (rows a0, a1, history pa) and pair B (rows b0, b1,
+// history pb). Row pairs (i0, i0 + 2^r) and (i0 + N/2, i0 + N/2 + 2^r) of a rank-K register tree have
+// the same lag at every step r <= K - 2, so one sm_100 packed f32x2 add does the work of two scalar
+// adds with the same rounding. The NORM multiplies stay scalar: packed multiplies by 1/sqrt2 here gave
+// outputs a few ulp from the scalar sequence on the GPU (the float32 parity tests at rank 16).
+template<bool NORM>
+__device__ __forceinline__ void bfly_x2(float &a0, float &a1, float &pa, float &b0, float &b1, float &pb, int L, int lane)
+{
+    const float xa = a0, xb = b0;
+    const float2 Y = make_float2(a1, b1);
+    const float2 A = (L == 0) ? make_float2(xa, xb) : make_float2(lagged(xa, pa, L, lane), lagged(xb, pb, L, lane));
+    const float2 Bl = make_float2(lagged(xa, pa, L + 1, lane), lagged(xb, pb, L + 1, lane));
+    float2 o0 = f2add(A, Y), o1 = f2add(Bl, Y);
+    if (NORM) {
+        o0 = make_float2(__fmul_rn(kRsqrt2, o0.x), __fmul_rn(kRsqrt2, o0.y));
+        o1 = make_float2(__fmul_rn(kRsqrt2, o1.x), __fmul_rn(kRsqrt2, o1.y));
+    }
+    a0 = o0.x; b0 = o0.y; a1 = o1.x; b1 = o1.y;
+    pa = xa; pb = xb;
+}
+
+// Step 0 with caller-supplied lag-1 operands (EXT0) for two pairs at once: (x, y) -> (x + y, e + y).
+template<bool NORM>
+__device__ __forceinline__ void bfly_ext0_x2(float &a0, float &a1, float ea, float &b0, float &b1, float eb)
+{
+    const float2 Y = make_float2(a1, b1);
+    float2 o0 = f2add(make_float2(a0, b0), Y), o1 = f2add(make_float2(ea, eb), Y);
+    if (NORM) {
+        o0 = make_float2(__fmul_rn(kRsqrt2, o0.x), __fmul_rn(kRsqrt2, o0.y));
+        o1 = make_float2(__fmul_rn(kRsqrt2, o1.x), __fmul_rn(kRsqrt2, o1.y));
+    }
+    a0 = o0.x; b0 = o0.y; a1 = o1.x; b1 = o1.y;
+}
+
 // All K steps of a register tree, in place. pv[r][q] holds pair q's row0 input of the previous tile.
 // With HS, the lag-0 pairs keep that history in shared memory (hs[slot], one float per pair, in
 // (r, q) order), which frees their registers. With EXT0, step 0 (all lags 0) takes its lag-1
@@ -823,25 +857,38 @@ __device__ __forceinline__ void rt_steps(float (&v)[RT<K>::N], float (&pv)[RT<K>
                                          const float *b0 = nullptr)
 {
     static_assert(!F0 || EXT0, "a caller-done step 0 keeps no history (EXT0 layout)");
+    constexpr int NP = RT<K>::NP, NH = RT<K>::N / 2;
     int slot = 0;
 #pragma unroll
     for (int r = 0; r < K; r++) {
 #pragma unroll
-        for (int q = 0; q < RT<K>::NP; q++) {
+        for (int q = 0; q < NP; q++) {
             const int h = 1 << r;
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
             const int L = rt_lag(r, q);
             if (F0 && r == 0)
                 continue;
+            // Packed: pair q < NP/2 with pair q + NP/2 (rows i0 + N/2), same lag, at steps r <= K - 2.
+            const bool PK = (K >= 2) && (r <= K - 2) && !(HS && L == 0 && !(EXT0 && r == 0));
+            if (PK && q >= NP / 2)
+                continue;   // done with its partner
             if (EXT0 && r == 0) {
-                const float x = v[i0], y = v[i0 + 1];
-                v[i0] = bfly_n<NORM>(x, y);
-                v[i0 + 1] = bfly_n<NORM>(b0[q], y);
+                if (PK) {
+                    bfly_ext0_x2<NORM>(v[i0], v[i0 + 1], b0[q], v[i0 + NH], v[i0 + NH + 1], b0[q + NP / 2]);
+                } else {
+                    const float x = v[i0], y = v[i0 + 1];
+                    v[i0] = bfly_n<NORM>(x, y);
+                    v[i0 + 1] = bfly_n<NORM>(b0[q], y);
+                }
                 continue;
             }
             if (HS && L == 0) {
                 bfly_l0_shared<NORM>(v[i0], v[i0 + h], hs + slot, lane);
                 slot++;
+                continue;
+            }
+            if (PK) {
+                bfly_x2<NORM>(v[i0], v[i0 + h], pv[r][q], v[i0 + NH], v[i0 + NH + h], pv[r][q + NP / 2], L, lane);
                 continue;
             }
             float x = v[i0], y = v[i0 + h];
@@ -946,14 +993,25 @@ __device__ __forceinline__ void phase_b_subbands(float (&v)[1 << RB], float (&pv
         }
 #pragma unroll
         for (int q = 0; q < RT<RB>::NP; q++) {
+            constexpr int NP = RT<RB>::NP, NH = NB / 2;
             const int i0 = ((q >> r) << (r + 1)) | (q & (h - 1));
             const int L = rt_lag(r, q);
-            if (F0 && r == 0) {
+            // packed pairs (q, q + NP/2) as in rt_steps
+            const bool PK = (RB >= 2) && (r <= RB - 2) && !(HS && L == 0 && !(EXT0 && r == 0)) && !(F0 && r == 0);
+            if (PK && q >= NP / 2) {
+                // done with its partner
+            } else if (F0 && r == 0) {
                 // done by the caller
             } else if (EXT0 && r == 0) {
-                const float x = v[i0], y = v[i0 + 1];
-                v[i0] = bfly_n<NORM>(x, y);
-                v[i0 + 1] = bfly_n<NORM>(b0[q], y);
+                if (PK) {
+                    bfly_ext0_x2<NORM>(v[i0], v[i0 + 1], b0[q], v[i0 + NH], v[i0 + NH + 1], b0[q + NP / 2]);
+                } else {
+                    const float x = v[i0], y = v[i0 + 1];
+                    v[i0] = bfly_n<NORM>(x, y);
+                    v[i0 + 1] = bfly_n<NORM>(b0[q], y);
+                }
+            } else if (PK) {
+                bfly_x2<NORM>(v[i0], v[i0 + h], pv[r][q], v[i0 + NH], v[i0 + NH + h], pv[r][q + NP / 2], L, lane);
             } else if (HS && L == 0) {
                 bfly_l0_shared<NORM>(v[i0], v[i0 + h], hs + slot, lane);
                 slot++;
