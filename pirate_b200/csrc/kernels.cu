@@ -1809,7 +1809,9 @@ template<typename Ts> __device__ __forceinline__ void pf_load8(const Ts *p, floa
 }
 
 // Shared-memory layout of the fast peak finder for one warp (see PfGeom).
-__host__ __device__ constexpr PfGeom pf_geom(int Dout, int Dcore, int tpad, int L, int esize)
+// LW: output times (lanes) per coarse DM in a warp (32, or 16 and 8 for trees with that few output
+// times per chunk: 32 / LW coarse DMs then share a warp).
+__host__ __device__ constexpr PfGeom pf_geom(int Dout, int Dcore, int tpad, int L, int esize, int LW = 32)
 {
     PfGeom g{};
     int off = 0;
@@ -1827,7 +1829,7 @@ __host__ __device__ constexpr PfGeom pf_geom(int Dout, int Dcore, int tpad, int 
         // blocks then fall on distinct banks for 8-byte loads); the others are stored contiguously.
         g.pad[l] = (pairs && nsamp >= 4) ? 2 : 0;
         g.I[l] = I;
-        g.n[l] = 32 * nsamp + I;
+        g.n[l] = LW * nsamp + I;
         g.dt[l] = dt;
         g.S[l] = (1 << l) / dt;
         g.nsamp[l] = nsamp;
@@ -1844,7 +1846,7 @@ __host__ __device__ constexpr PfGeom pf_geom(int Dout, int Dcore, int tpad, int 
             off += (size + 1) & ~1;
     }
     g.raw_off = (off + 3) & ~3;
-    g.raw_floats = ((32 * Dout + tpad) * esize + 15) / 16 * 4;
+    g.raw_floats = ((LW * Dout + tpad) * esize + 15) / 16 * 4;
     g.w_off = g.raw_off + 2 * g.raw_floats;
     g.warp_floats = g.w_off + kPfMaxProfiles * 32;
     return g;
@@ -1860,21 +1862,26 @@ __host__ __device__ constexpr int pf_tpad_of(int L) { return (2 << L) > 4 ? (2 <
 // where the level is only known at run time.
 // CTR: the chunk index comes from the device counter (replayed CUDA graphs). It is a template flag
 // because reading it costs the kernel about 26 registers, which the direct launches should not pay.
-template<typename Ts, int L, int DOUT, bool CTR>
+template<typename Ts, int L, int DOUT, bool CTR, int LW>
 __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, const PfGeom &gr)
 {
+    static_assert(LW == 32 || LW == 16 || LW == 8, "lanes per coarse DM");
+    constexpr int G = 32 / LW;   // coarse DMs per warp, each on LW consecutive lanes
     extern __shared__ float sm[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int dm = blockIdx.y * kPfWarps + warp;
+    const int warp = threadIdx.x >> 5, sub = (threadIdx.x & 31) / LW, lane = threadIdx.x & (LW - 1);
+    const int dm0 = (blockIdx.y * kPfWarps + warp) * G;
     const int b = blockIdx.z, bt = a.beam0 + b;
-    const int tout0 = blockIdx.x * 32;
-    if (dm >= a.ndm_out)
+    const int tout0 = blockIdx.x * LW;
+    if (dm0 >= a.ndm_out)
         return;   // whole warp exits; warps never synchronize across the block
+    // A sub-group past the last coarse DM computes the last one again and stores nothing.
+    const bool dm_ok = dm0 + sub < a.ndm_out;
+    const int dm = dm_ok ? dm0 + sub : a.ndm_out - 1;
 
-    const int ntw = min(32, a.nt_out - tout0);
+    const int ntw = min(LW, a.nt_out - tout0);
     const int tout = tout0 + lane;
-    const bool active = (lane < ntw);
-    float *lev = sm + warp * g.warp_floats;
+    const bool active = (lane < ntw) && dm_ok;
+    float *lev = sm + (warp * G + sub) * g.warp_floats;
 
     const int Dout = (DOUT > 0) ? DOUT : a.Dout;
     const int tpad = (DOUT > 0) ? pf_tpad_of(L) : a.tpad;
@@ -1883,8 +1890,8 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
     // as wsm[p * 32 + j] (lanes of one weight time read the same word, consecutive weight times
     // consecutive words), and reloaded only when a multiplet's subband differs from the previous one.
     const float *wrow = a.wt + ((long) b * a.ndm_wt + dm / Wds) * a.nt_wt * a.P * a.N;
-    const int tw0 = tout0 / Tds, NT = (Tds >= 32) ? 1 : 32 / Tds;
-    const int tl = active ? (tout / Tds - tw0) : 0;
+    const int tw0 = tout0 / Tds, NT = (Tds >= LW) ? 1 : LW / Tds;
+    const int tl = (lane < ntw) ? (tout / Tds - tw0) : 0;
     float *wsm = lev + g.w_off;
     int wsm_n = -1;
     const Ts *pfrows = (const Ts *) a.pf + ((long) bt * a.ndm_out + dm) * a.M * a.pf_cap;
@@ -1914,7 +1921,7 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
     auto stage = [&](int m) {
         const Ts *row = pfrows + (long) m * a.pf_cap;
         Ts *raw = raw0 + (m & 1) * raw_ts;
-        for (int q = lane; q < nq0; q += 32)
+        for (int q = lane; q < nq0; q += LW)
             cp_async_bytes<4 * sizeof(Ts)>(raw + 4 * q, row + ((sbm + 4 * q) & mask));
         cp_async_commit();
     };
@@ -1931,7 +1938,7 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
 
         const int n = a.m_to_n[m];
         if (n != wsm_n) {
-            for (int idx = lane; idx < a.P * NT; idx += 32) {
+            for (int idx = lane; idx < a.P * NT; idx += LW) {
                 const int p = idx / NT, j = idx - p * NT, t = tw0 + j;
                 wsm[p * 32 + j] = (t < a.nt_wt) ? wrow[((long) t * a.P + p) * a.N + n] : 0.0f;
             }
@@ -1947,13 +1954,13 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
             if (l > 0 && !U) {
                 // Saturated level (dt = Dcore): B_l[u] = B_{l-1}[rr u] + B_{l-1}[rr u + ss].
                 const int rr = g.rr[l], ss = g.ss[l];
-                for (int u = lane; u < g.n[l]; u += 32)
+                for (int u = lane; u < g.n[l]; u += LW)
                     lev[pf_phys(g, l, u)] = __fadd_rn(lev[pf_phys(g, l - 1, rr * u)], lev[pf_phys(g, l - 1, rr * u + ss)]);
                 __syncwarp();
             }
             if (nextU) {
                 // Entries of level l+1 before the first output time.
-                for (int u = lane; u < g.I[l + 1]; u += 32)
+                for (int u = lane; u < g.I[l + 1]; u += LW)
                     lev[pf_phys(g, l + 1, u)] = (l == 0) ? __fadd_rn(to_f(rawc[2 * u]), to_f(rawc[2 * u + 1]))
                                                         : __fadd_rn(lev[pf_phys(g, l, 2 * u)], lev[pf_phys(g, l, 2 * u + 1)]);
             }
@@ -2150,14 +2157,14 @@ __device__ __forceinline__ void pf_fast_body(const PfArgs &a, const PfGeom &g, c
 
 // DOUT > 0: compiled for that output time downsampling (with Dcore = min(DOUT, 8) and the plan's tpad
 // for L levels); DOUT = 0: any Dout >= 4, geometry read from the launch arguments.
-template<typename Ts, int L, int DOUT, bool CTR>
+template<typename Ts, int L, int DOUT, bool CTR, int LW = 32>
 __global__ void __launch_bounds__(kPfWarps * 32) pf_fast_kernel(PfArgs a, PfGeom gr)
 {
     if constexpr (DOUT > 0) {
-        constexpr PfGeom gc = pf_geom(DOUT, pf_dcore_of(DOUT), pf_tpad_of(L), L, sizeof(Ts));
-        pf_fast_body<Ts, L, DOUT, CTR>(a, gc, gr);
+        constexpr PfGeom gc = pf_geom(DOUT, pf_dcore_of(DOUT), pf_tpad_of(L), L, sizeof(Ts), LW);
+        pf_fast_body<Ts, L, DOUT, CTR, LW>(a, gc, gr);
     } else {
-        pf_fast_body<Ts, L, 0, CTR>(a, gr, gr);
+        pf_fast_body<Ts, L, 0, CTR, LW>(a, gr, gr);
     }
 }
 
@@ -2318,17 +2325,19 @@ static bool pf_fast_ok(const PfArgs &a)
     return !a.force_general && a.Dout >= 4 && (a.tpad % 4) == 0 && (s0 % 4) == 0 && (a.pf_cap % 4) == 0 && a.L <= 5 && a.P <= kPfMaxProfiles;
 }
 
-template<typename Ts, int L, int DOUT>
+template<typename Ts, int L, int DOUT, int LW = 32>
 static void launch_pf_fast(const PfArgs &a, const PfGeom &g, int B, cudaStream_t s)
 {
-    size_t sm = (size_t) kPfWarps * g.warp_floats * sizeof(float);
-    dim3 grid((a.nt_out + 31) / 32, (a.ndm_out + kPfWarps - 1) / kPfWarps, B);
+    // g: the geometry for LW lanes per coarse DM
+    constexpr int G = 32 / LW;
+    size_t sm = (size_t) kPfWarps * G * g.warp_floats * sizeof(float);
+    dim3 grid((a.nt_out + LW - 1) / LW, (a.ndm_out + kPfWarps * G - 1) / (kPfWarps * G), B);
     if (a.chunk_ctr) {
-        set_smem(pf_fast_kernel<Ts, L, DOUT, true>, sm);
-        pf_fast_kernel<Ts, L, DOUT, true><<<grid, kPfWarps * 32, sm, s>>>(a, g);
+        set_smem(pf_fast_kernel<Ts, L, DOUT, true, LW>, sm);
+        pf_fast_kernel<Ts, L, DOUT, true, LW><<<grid, kPfWarps * 32, sm, s>>>(a, g);
     } else {
-        set_smem(pf_fast_kernel<Ts, L, DOUT, false>, sm);
-        pf_fast_kernel<Ts, L, DOUT, false><<<grid, kPfWarps * 32, sm, s>>>(a, g);
+        set_smem(pf_fast_kernel<Ts, L, DOUT, false, LW>, sm);
+        pf_fast_kernel<Ts, L, DOUT, false, LW><<<grid, kPfWarps * 32, sm, s>>>(a, g);
     }
     check_launch("pf_fast_kernel");
 }
@@ -2340,6 +2349,19 @@ static void launch_pf_l(const PfArgs &a, int B, cudaStream_t s)
         const PfGeom g = pf_geom(a.Dout, a.Dcore, a.tpad, L, (int) sizeof(Ts));
         // Compiled geometries for the usual output downsamplings (pirate's default Dout = 2^pf_rank).
         const bool std_geom = (a.Dcore == pf_dcore_of(a.Dout)) && (a.tpad == pf_tpad_of(L));
+        // Trees with 16 or 8 output times per chunk (the most downsampled primary trees) share a warp
+        // between 2 or 4 coarse DMs, so that no lane idles (compiled for the benchmark's Dout 16, widths
+        // to 32).
+        if constexpr (L == 5) {
+            if (std_geom && a.Dout == 16 && a.nt_out <= 8) {
+                launch_pf_fast<Ts, L, 16, 8>(a, pf_geom(a.Dout, a.Dcore, a.tpad, L, (int) sizeof(Ts), 8), B, s);
+                return;
+            }
+            if (std_geom && a.Dout == 16 && a.nt_out <= 16) {
+                launch_pf_fast<Ts, L, 16, 16>(a, pf_geom(a.Dout, a.Dcore, a.tpad, L, (int) sizeof(Ts), 16), B, s);
+                return;
+            }
+        }
         if (std_geom && a.Dout == 16) launch_pf_fast<Ts, L, 16>(a, g, B, s);
         else if (std_geom && a.Dout == 8) launch_pf_fast<Ts, L, 8>(a, g, B, s);
         else if (std_geom && a.Dout == 4) launch_pf_fast<Ts, L, 4>(a, g, B, s);

@@ -123,6 +123,26 @@ def test_fp32_bitwise_rank16(pb2lib):
             assert np.array_equal(gres[seq][1][i], ores[seq][1][i]), "seq %d tree %d out_argmax" % (seq, i)
 
 
+def test_fp32_small_output_trees_share_warps(pb2lib):
+    """Rank 14, 5 primary trees, peak-finding downsampling 16: the two most downsampled trees have 16 and
+    8 output times per chunk, and their peak finder runs 2 and 4 coarse DMs per warp (16 and 8 lanes
+    each). Two beams, three chunks, NaN planted in one beam: bitwise the fp32 oracle."""
+    import bench
+    cfg = bench.bench_config(2, "float32", 14, 5, 4096)
+    plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(cfg))
+    assert [t.nt_out for t in plan.trees][-2:] == [16, 8]
+    xs = H.make_inputs(cfg, 3, seed=14)
+    xs[1][1, 100:140, 500:520] = np.nan
+    orc, _ = H.run_oracle(cfg, xs[:0], [])
+    ws = H.make_weights(orc, seed=14)
+    _, ores = H.run_oracle(cfg, xs, ws, 1, 32)
+    _, _, gres = H.run_gpu(pb2lib, cfg, xs, ws)
+    for seq in range(len(xs)):
+        for i in range(orc.ntrees):
+            assert np.array_equal(gres[seq][0][i], ores[seq][0][i], equal_nan=True), "seq %d tree %d out_max" % (seq, i)
+            assert np.array_equal(gres[seq][1][i], ores[seq][1][i]), "seq %d tree %d out_argmax" % (seq, i)
+
+
 @pytest.mark.parametrize("dtype", ["float32", "float16"])
 def test_benchmark_config_full_size(pb2lib, dtype):
     """The benchmark's workload at full size, one beam, two chunks, fed pirate's raw int4 input
