@@ -1259,10 +1259,10 @@ __global__ void __launch_bounds__(32 * ((1 << RA) + (1 << RB)), 1) tree_kernel(c
     constexpr bool FB = (STAGE == 2) && !STAG && (RB >= 1);
     constexpr bool EB = E0 || FB;
     // bfly_n per phase: float32 storage normalizes every step. 16-bit storage skips the 1/sqrt2 in both
-    // phases of stage 1 and in phase a of stage 2 (measured 4% and 2% faster), not in stage 2's
-    // phase b (3% slower there), and scales by tree_scale(SU) where values leave the registers.
+    // phases of both stages (measured 4%, 2% and, with the packed adds, 2% faster in stage 2's phase b)
+    // and scales by tree_scale(SU) where values leave the registers.
     constexpr bool NORM_A = (sizeof(Ts) == 4);
-    constexpr bool NORM_B = (sizeof(Ts) == 4) || (STAGE == 2);
+    constexpr bool NORM_B = (sizeof(Ts) == 4);
     constexpr int SA = NORM_A ? 0 : RA;                 // unnormalized steps before phase b
     constexpr int SU = SA + (NORM_B ? 0 : RB);          // ... and after it
     const int b = blockIdx.y, bt = a.beam0 + b;
