@@ -179,6 +179,11 @@ def run_ours(args, rank, world):
 
     dq_data, dq_so = quantized_input("cuda")
 
+    # The consumer acquires and releases outputs on its own stream (as pirate's timing loop does on its
+    # kernel-timer stream): on the input stream, the next chunk's launch would wait for this chunk's
+    # outputs, leaving a gap between consecutive chunks' kernels.
+    out_dev = torch.cuda.Stream()
+
     def step_device():
         """One chunk of all beams (nbat batches); the int4 input stays resident in the input slots."""
         s0 = seq[0]
@@ -189,8 +194,8 @@ def run_ours(args, rank, world):
                 so.copy_(dq_so)
             dd.release_input_and_launch_dd_kernels(s, stream)
         for s in range(s0, s0 + nbat):
-            dd.acquire_output(0, s, stream)
-            dd.release_output(0, s, stream)
+            dd.acquire_output(0, s, out_dev)
+            dd.release_output(0, s, out_dev)
         seq[0] += nbat
 
     for _ in range(args.warmup):
@@ -199,7 +204,7 @@ def run_ours(args, rank, world):
     replicas.barrier()
     torch.cuda.synchronize()
 
-    dd.enable_timing(True)
+    # Timed region: K steps bracketed by events on the caller stream (the headline).
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clk:
@@ -207,14 +212,30 @@ def run_ours(args, rank, world):
         e0.record(stream)
         for _ in range(args.steps):
             step_device()
+        stream.wait_stream(out_dev)   # the last chunk's outputs consumed
         e1.record(stream)
         torch.cuda.synchronize()
         clk.mark(h0, time.time())
-    ktimes = dd.kernel_times()
-    dd.enable_timing(False)
     ms = replicas.max_over_ranks(e0.elapsed_time(e1))
     replicas.barrier()
     ms_per_step = ms / args.steps
+    # A second timed region of K steps with CUDA events around every kernel class on the dedisperser's
+    # compute stream (the roofline's per-kernel durations). The events between the kernels cost about
+    # 2-3% of a step, so they stay out of the headline region.
+    torch.cuda.synchronize()
+    dd.enable_timing(True)
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for _ in range(args.steps):
+        step_device()
+    stream.wait_stream(out_dev)
+    k1.record(stream)
+    torch.cuda.synchronize()
+    ktimes = dd.kernel_times()
+    dd.enable_timing(False)
+    kms_per_step = replicas.max_over_ranks(k0.elapsed_time(k1)) / args.steps
+    replicas.barrier()
 
     # End to end through the public API, as pirate's timing loop (GpuDedisperser::time,
     # src_lib/GpuDedisperser.cpp:1584-1680) runs it: per step, the int4 data and scales/offsets go from
@@ -271,6 +292,15 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     ems = replicas.max_over_ranks(f0.elapsed_time(f1))
 
+    # pirate's own timing loop through the C ABI (GpuDedisperser::time: int4 batches from pinned host
+    # memory, kernels, output consumed): beams_per_batch * chunk seconds over the interval between
+    # consecutive batches' completions, median after 2 * nbat warm-up iterations (rank 0's GPU).
+    torch.cuda.synchronize()
+    nit = max(4 * nbat + 2, min(args.steps, 40))
+    rtb = dd.time(nit)
+    time_loop = float(np.median(rtb[2 * nbat + 1:]))
+    seq[0] += nit
+
     # Beams whose state fits in this GPU's HBM at this plan: total memory over the device bytes per beam.
     per_beam = dd.device_bytes() / float(args.beams)
     capacity_beams = int(torch.cuda.get_device_properties(dev).total_memory // per_beam)
@@ -279,6 +309,7 @@ def run_ours(args, rank, world):
     # The gridding class reads int4 data and scales/offsets instead of storage-dtype samples.
     alg[0] += float(args.beams) * plan.nfreq * (plan.nt_in / 2 + plan.nt_in / 256 * 4 - plan.nt_in * esize)
     return dict(plan=plan, dd=dd, ms_per_step=ms_per_step, e2e_ms_per_step=ems / e2e_steps, ktimes=ktimes,
+                kms_per_step=kms_per_step, time_loop=time_loop, time_loop_iters=nit,
                 alg=alg, clocks=clk.summary(), h2d=h2d, d2h=d2h, device_bytes=dd.device_bytes(),
                 kernels_per_batch=dd.kernels_per_batch() * nbat, capacity_beams=capacity_beams,
                 bytes_per_beam=per_beam)
@@ -447,6 +478,7 @@ def run_plain_fp32(args, steps):
     g.manual_seed(99)
     x = torch.randn((1, plan.nfreq, plan.nt_in), generator=g, device="cuda", dtype=torch.float32)
     seq = [0]
+    out = torch.cuda.Stream()   # outputs consumed on their own stream, as in the headline loop
 
     def step():
         s = seq[0]
@@ -454,8 +486,8 @@ def run_plain_fp32(args, steps):
         if s == 0:
             a.copy_(x)
         dd.release_input_and_launch_dd_kernels(s, stream)
-        dd.acquire_output(0, s, stream)
-        dd.release_output(0, s, stream)
+        dd.acquire_output(0, s, out)
+        dd.release_output(0, s, out)
         seq[0] += 1
 
     for _ in range(3):
@@ -466,6 +498,7 @@ def run_plain_fp32(args, steps):
     e0.record(stream)
     for _ in range(steps):
         step()
+    stream.wait_stream(out)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
@@ -676,6 +709,11 @@ def main():
                 "kernels": {c: {"ms_per_step": round(kt[c][0] / nsteps, 4), "share": round(kt[c][0] / tot_ms, 4) if tot_ms else None,
                                 "alg_GBps": round(r["alg"][i] / (kt[c][0] / nsteps * 1e-3) / 1e9, 1) if kt[c][0] else None}
                             for i, c in enumerate(classes)},
+                "time_loop": {"value": round(r["time_loop"], 2), "unit": "beams", "iterations": r["time_loop_iters"],
+                              "note": "pirate's GpuDedisperser::time loop (pb2_dd_time) on one GPU: int4 input copied from "
+                                      "pinned host memory every batch, median over iterations"},
+                "kernel_timing": {"ms_per_step": round(r["kms_per_step"], 4), "steps": nsteps,
+                                  "note": "per-kernel-class CUDA events in a second timed region of the same K steps"},
                 "pipeline_alg_GBps": round(e2e_alg_gbs, 1),
                 "device_bytes": r["device_bytes"],
                 "clocks": r["clocks"]}

@@ -218,6 +218,15 @@ int pb2_dd_fill_weights(pb2_dedisperser *dd, long itree, const float *host, long
 int pb2_dd_fill_analytic_weights(pb2_dedisperser *dd, const double *freq_variances, long nfreq);
 /* GpuDedisperser::stop, src_lib/GpuDedisperser.cpp:735 */
 int pb2_dd_stop(pb2_dedisperser *dd);
+/* GpuDedisperser::time, src_lib/GpuDedisperser.cpp:1573-1665: pirate's timing loop over niterations
+ * batches. Each copies one batch of int4 data and fp16 (scale, offset) pairs from pinned host memory into
+ * the acquired int4 input slot on a copy stream, launches the kernels (dequantization fused into
+ * gridding) and acquires and releases the output as consumer 0. rtb[i] (niterations doubles) receives
+ * iteration i's real-time beams, beams_per_batch * chunk seconds / (time between the completions of
+ * iterations i-1 and i); rtb[0] = 0. pirate prints the same figure per iteration. Needs num_consumers 1,
+ * time_samples_per_chunk a multiple of 256, niterations > 2 * num_active_batches, and no acquired
+ * batch left unreleased; the seq_id cursors advance by niterations. */
+int pb2_dd_time(pb2_dedisperser *dd, long niterations, double *rtb);
 /* Clears every delay line and tree state (and the input and output slots) on 'stream', after waiting for
  * the batches already launched: later chunks see zeros as their history, as at the start of a stream.
  * The seq_id cursors are unchanged. (No pirate counterpart; used to separate synthetic events.) */

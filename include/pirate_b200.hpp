@@ -6,7 +6,7 @@
 //   pirate::DedispersionPlan     include/pirate/DedispersionPlan.hpp:33-225 (trees, decode_argmax)
 //   pirate::GpuDedisperser       include/pirate/Dedisperser.hpp:45-254 (create, allocate, acquire_input,
 //                                release_input_and_launch_dd_kernels, acquire_output -> Outputs by value,
-//                                release_output, fill_all_weights, fill_analytic_weights, stop)
+//                                release_output, fill_all_weights, fill_analytic_weights, stop, time)
 // Errors are thrown as std::runtime_error carrying the library's message, as pirate's xassert does.
 // Streams are cudaStream_t values passed as void * (nullptr: the legacy default stream), so this
 // header needs no CUDA headers.
@@ -170,6 +170,14 @@ public:
         check(pb2_dd_fill_analytic_weights(h, freq_variances.data(), long(freq_variances.size())));
     }
     void stop() { check(pb2_dd_stop(h)); }
+    // GpuDedisperser::time (src_lib/GpuDedisperser.cpp:1573-1665): the real-time beams of each of
+    // niterations int4 batches copied from pinned host memory, dedispersed and consumed (element 0 is 0).
+    std::vector<double> time(long niterations)
+    {
+        std::vector<double> rtb(niterations > 0 ? niterations : 0);
+        check(pb2_dd_time(h, niterations, rtb.data()));
+        return rtb;
+    }
     long device_bytes() const
     {
         long n = 0;

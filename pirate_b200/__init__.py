@@ -114,6 +114,7 @@ def lib():
         "pb2_sifter_train_step": (ctypes.c_int, [vp, vp, vp, ctypes.c_long, ctypes.c_float, dp, vp]),
         "pb2_dd_enable_sifter": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pb2_dd_zero_state": (ctypes.c_int, [vp, vp]),
+        "pb2_dd_time": (ctypes.c_int, [vp, ctypes.c_long, dp]),
         "pb2_batched_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_long, ctypes.c_int, ctypes.POINTER(vp)]),
         "pb2_batched_allocate": (ctypes.c_int, [vp]),
         "pb2_batched_ngroups": (ctypes.c_int, [vp, lp]),
@@ -521,6 +522,16 @@ class GpuDedisperser:
 
     def stop(self):
         _check(lib().pb2_dd_stop(self._h))
+
+    def time(self, niterations):
+        """pirate's GpuDedisperser.time (src_lib/GpuDedisperser.cpp:1573-1665): int4 batches copied from
+        pinned host memory, dedispersed and consumed in a loop; returns the real-time beams of every
+        iteration (numpy array; element 0 is 0, the first 2 * num_active_batches are warm-up)."""
+        out = np.zeros(int(niterations), np.float64)
+        _check(lib().pb2_dd_time(self._h, int(niterations), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        self._next_in += int(niterations)
+        self._next_out = [n + int(niterations) for n in self._next_out]
+        return out
 
     def zero_state(self, stream=None):
         """Clears every delay line and tree state (later chunks see zeros as history); the seq_id

@@ -519,6 +519,11 @@ int pb2_dd_stop(pb2_dedisperser *dd)
     return guard([&] { REQUIRE_PTR(dd); dd->d->stop(); });
 }
 
+int pb2_dd_time(pb2_dedisperser *dd, long niterations, double *rtb)
+{
+    return guard([&] { REQUIRE_PTR(dd); REQUIRE_PTR(rtb); dd->d->time(niterations, rtb); });
+}
+
 int pb2_dd_zero_state(pb2_dedisperser *dd, void *stream)
 {
     return guard([&] { REQUIRE_PTR(dd); dd->d->zero_state((cudaStream_t) stream); });

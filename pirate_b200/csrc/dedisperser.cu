@@ -924,6 +924,92 @@ void GpuDedisperser::fill_all_weights(long itree, const float *host, long nelts)
     });
 }
 
+void GpuDedisperser::time(long niterations, double *rtb)
+{
+    const long seq0 = entry([&]() -> long {
+        if (!allocated) throw runtime_error("GpuDedisperser::time(): allocate() was not called");
+        if (!d_qdata.ptr) throw runtime_error("GpuDedisperser::time(): time_samples_per_chunk must be a multiple of 256");
+        if (params.num_consumers != 1) throw runtime_error("GpuDedisperser::time(): needs num_consumers == 1");
+        if (niterations <= 2 * nstreams)
+            throw runtime_error("GpuDedisperser::time(): niterations must be > 2 * num_active_batches");
+        if (!rtb) throw runtime_error("GpuDedisperser::time(): null output array");
+        if (next_acq_in != next_rel_in || next_acq_out[0] != next_rel_in || next_rel_out[0] != next_rel_in)
+            throw runtime_error("GpuDedisperser::time(): every launched batch must have been consumed first");
+        return next_acq_in;
+    });
+    CUDA_CHECK(cudaSetDevice(params.cuda_device_id));
+    const long S = nstreams, K = nstreams + 2;
+    const size_t data_bytes = size_t(B) * plan.nfreq * (plan.nt_in / 2);
+    const size_t so_bytes = size_t(B) * plan.nfreq * (plan.nt_in / 256) * 2 * sizeof(uint16_t);
+    const double chunk_seconds = 1.0e-3 * plan.nt_in * plan.config.time_sample_ms;
+
+    // Resources of the loop, released on every exit path.
+    struct Res
+    {
+        std::vector<void *> host;
+        cudaStream_t h2g = nullptr, tstream = nullptr;
+        std::vector<cudaEvent_t> ev;
+        ~Res()
+        {
+            if (h2g) cudaStreamSynchronize(h2g);
+            if (tstream) cudaStreamSynchronize(tstream);
+            for (void *p : host) cudaFreeHost(p);
+            for (cudaEvent_t e : ev) cudaEventDestroy(e);
+            if (h2g) cudaStreamDestroy(h2g);
+            if (tstream) cudaStreamDestroy(tstream);
+        }
+    } r;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&r.h2g, cudaStreamNonBlocking));
+    CUDA_CHECK(cudaStreamCreateWithFlags(&r.tstream, cudaStreamNonBlocking));
+    r.ev.assign(K, nullptr);
+    for (auto &e : r.ev) CUDA_CHECK(cudaEventCreate(&e));
+    // One host copy of the raw data per compute stream, as pirate's multi_raw_cpu: seeded pseudo-random
+    // nibbles (values -8..7, the missing-sample code among them), scale 0.5 and offset 0 per 256
+    // samples. (Timing depends a little on the data: the peak finder does more work where maxima move.)
+    uint64_t x = 0x9e3779b97f4a7c15ULL;
+    for (long i = 0; i < S; i++) {
+        void *d = nullptr, *so = nullptr;
+        CUDA_CHECK(cudaHostAlloc(&d, data_bytes, cudaHostAllocDefault));
+        r.host.push_back(d);
+        CUDA_CHECK(cudaHostAlloc(&so, so_bytes, cudaHostAllocDefault));
+        r.host.push_back(so);
+        uint64_t *w = (uint64_t *) d;
+        for (size_t j = 0; j < data_bytes / 8; j++) {
+            x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+            w[j] = x;
+        }
+        uint16_t *h = (uint16_t *) so;
+        for (size_t j = 0; j < so_bytes / 2; j += 2) { h[j] = 0x3800; h[j + 1] = 0; }   // fp16 0.5, 0
+    }
+
+    for (long i = 0; i < niterations; i++) {
+        const long seq = seq0 + i;
+        void *so = nullptr;
+        void *data = acquire_input_int4(seq, r.h2g, &so);
+        CUDA_CHECK(cudaMemcpyAsync(data, r.host[2 * (i % S)], data_bytes, cudaMemcpyHostToDevice, r.h2g));
+        CUDA_CHECK(cudaMemcpyAsync(so, r.host[2 * (i % S) + 1], so_bytes, cudaMemcpyHostToDevice, r.h2g));
+        release_input_and_launch_dd_kernels(seq, r.h2g);
+        acquire_output(0, seq, r.tstream, false);
+        release_output(0, seq, r.tstream);
+        CUDA_CHECK(cudaEventRecord(r.ev[i % K], r.tstream));
+        // Completion times lag the launches by S iterations, as pirate's KernelTimer.
+        const long j = i - S;
+        if (j >= 1) {
+            CUDA_CHECK(cudaEventSynchronize(r.ev[j % K]));
+            float ms = 0;
+            CUDA_CHECK(cudaEventElapsedTime(&ms, r.ev[(j - 1) % K], r.ev[j % K]));
+            rtb[j] = B * chunk_seconds / (1.0e-3 * ms);
+        }
+    }
+    rtb[0] = 0.0;
+    for (long j = std::max(1L, niterations - S); j < niterations; j++) {
+        CUDA_CHECK(cudaEventSynchronize(r.ev[j % K]));
+        float ms = 0;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, r.ev[(j - 1) % K], r.ev[j % K]));
+        rtb[j] = B * chunk_seconds / (1.0e-3 * ms);
+    }
+}
+
 // GpuDedisperser::fill_analytic_weights (src_lib/GpuDedisperser.cpp:1162-1238): one beam's weights
 // per tree from the analytic variances, copied to every (weight batch, beam) slot on the compute stream.
 void GpuDedisperser::fill_analytic_weights(const double *freq_variances, long nfreq)

@@ -125,6 +125,15 @@ public:
     // later chunks see zeros as their history). Waits for this object's launched batches first.
     void zero_state(cudaStream_t stream);
 
+    // pirate's timing loop (GpuDedisperser::time, src_lib/GpuDedisperser.cpp:1573-1665): niterations
+    // batches, each copying one batch of int4 data and fp16 (scale, offset) pairs from pinned host
+    // memory into the acquired int4 input slot on a copy stream, launching the kernels (dequantization
+    // fused into gridding), and acquiring and releasing the output as consumer 0. rtb[i] receives the
+    // real-time beams of iteration i: beams_per_batch * chunk seconds / (time between the completions
+    // of iterations i-1 and i); rtb[0] = 0. Needs num_consumers == 1, nt_in a multiple of 256,
+    // niterations > 2 * num_active_batches, and every cursor caught up (nothing acquired and unreleased).
+    void time(long niterations, double *rtb);
+
     // Device bytes held by allocate() (for reporting).
     size_t device_bytes() const { return total_bytes; }
     // Pinned host bytes of the spilled delay lines (rows whose readers are more than the config's

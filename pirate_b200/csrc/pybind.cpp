@@ -123,5 +123,6 @@ PYBIND11_MODULE(_pirate_b200_pybind, m)
                 py::gil_scoped_release nogil;
                 d.fill_analytic_weights(v);
             }, py::arg("freq_variances"))
+        .def("time", &GpuDedisperser::time, py::arg("niterations"), py::call_guard<py::gil_scoped_release>())
         .def("stop", &GpuDedisperser::stop);
 }

@@ -234,3 +234,52 @@ def test_batches_overlap_on_two_compute_streams(pb2lib):
             assert not out.candidates["valid"].cpu().numpy().any()
             dd.release_output(0, seq)
     torch.cuda.synchronize()
+
+
+def _time_cfg(**kw):
+    return H.toy_config(rank=8, nfreq=300, nt=512, dtype="float16", subbands=[2, 2, 1], beams_per_gpu=4,
+                        beams_per_batch=2, num_active_batches=kw.pop("num_active_batches", 2))
+
+
+def test_time_loop(pb2lib):
+    """pirate's GpuDedisperser.time: int4 batches from pinned host memory through the public entry
+    points, on two compute streams. Every iteration after the first reports a positive, finite real-time
+    beam count; the cursors advance, so the streaming API carries on from seq_id = niterations, and the
+    pybind11 surface runs the same loop."""
+    import torch
+    cfg = _time_cfg()
+    plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(cfg))
+    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=1)
+    dd.allocate()
+    dd.fill_analytic_weights(np.ones(plan.nfreq))
+    rtb = dd.time(12)
+    assert rtb.shape == (12,) and rtb[0] == 0
+    assert np.all(np.isfinite(rtb[1:])) and np.all(rtb[1:] > 0)
+    with dd.get_input() as x:          # seq_id 12
+        x.zero_()
+    with dd.get_output(0, sync=True) as out:
+        assert out.ichunk_zero_based == 6 and out.ibeam == 0
+    torch.cuda.synchronize()
+
+    from pirate_b200 import _pirate_b200_pybind as pyb
+    c = pyb.DedispersionConfig.from_yaml_string(pb2lib.DedispersionConfig.from_dict(cfg).to_yaml_string())
+    d2 = pyb.GpuDedisperser(pyb.DedispersionPlan(c), cuda_device_id=0, num_consumers=1)
+    d2.allocate()
+    r2 = np.array(d2.time(6))
+    assert r2[0] == 0 and np.all(r2[1:] > 0)
+
+
+def test_time_loop_preconditions(pb2lib):
+    """time() needs one consumer and more than 2 * num_active_batches iterations; a failing call stops
+    the dedisperser, as pirate's entry points do."""
+    cfg = _time_cfg()
+    plan = pb2lib.DedispersionPlan(pb2lib.DedispersionConfig.from_dict(cfg))
+    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=2)
+    dd.allocate()
+    with pytest.raises(RuntimeError, match="num_consumers == 1"):
+        dd.time(8)
+    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=1)
+    dd.allocate()
+    with pytest.raises(RuntimeError, match="niterations"):
+        dd.time(4)
+    _stopped(dd)
