@@ -235,7 +235,7 @@ int pb2_dd_zero_state(pb2_dedisperser *dd, void *stream);
  * kernel classes [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf]. */
 int pb2_dd_kernels_per_batch(const pb2_dedisperser *dd, long *n);
 int pb2_dd_algorithmic_bytes(const pb2_dedisperser *dd, double *out5);
-/* Per-kernel-class CUDA-event timing on the dedisperser's compute stream (the analogue of pirate's
+/* Per-kernel-class CUDA-event timing on the dedisperser's compute streams (the analogue of pirate's
  * KernelTimer / ResourceTracker reporting, src_lib/GpuDedisperser.cpp:1674-1681). kernel_times()
  * synchronizes and returns accumulated milliseconds and launch counts for [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf]. */
 int pb2_dd_enable_timing(pb2_dedisperser *dd, int on);
@@ -267,7 +267,7 @@ int pb2_sifter_train_step(pb2_sifter *s, const void *patches, const float *label
                           void *stream);
 /* Adds the candidate stage to every later batch of 'dd' (after pb2_dd_allocate): per-beam peak over the
  * trees, patches of peaks >= threshold (sigma), and scores by 'sifter' (may be null: scores are then the
- * peaks). The results appear in pb2_outputs. The sifter then runs on the dedisperser's compute stream
+ * peaks). The results appear in pb2_outputs. The sifter then runs on the dedisperser's compute streams
  * and must neither be trained meanwhile nor destroyed before the dedisperser. */
 int pb2_dd_enable_sifter(pb2_dedisperser *dd, float threshold, pb2_sifter *sifter);
 

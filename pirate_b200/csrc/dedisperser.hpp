@@ -107,9 +107,9 @@ public:
     // per-channel input variances (nfreq values > 0), and waits until they are on the GPU.
     void fill_analytic_weights(const double *freq_variances, long nfreq);
     void stop(std::exception_ptr e = nullptr);
-    // Adds the candidate stage to every later batch, on the compute stream after peak finding: the
+    // Adds the candidate stage to every later batch, on its compute stream after peak finding: the
     // per-beam peak over the trees, the candidate patch of peaks >= threshold, and (if 'sifter' is not
-    // null) its MLP score. Requires allocate(). The sifter is used on the compute stream from then on
+    // null) its MLP score. Requires allocate(). The sifter is used on the compute streams from then on
     // and must not be trained at the same time; it must outlive the dedisperser or a later
     // enable_sifter() call.
     void enable_sifter(float threshold, Sifter *sifter);
@@ -148,7 +148,7 @@ public:
     std::vector<double> algorithmic_bytes() const;
 
     // Kernel timing: when enabled, CUDA events bracket each kernel class
-    // [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf] on the compute stream; kernel_times() synchronizes and returns
+    // [grid+lds (one fused kernel), candidates+sifter, stage1, stage2, pf] on the batch's compute stream; kernel_times() synchronizes and returns
     // the accumulated milliseconds and launch counts since the last reset.
     void enable_timing(bool on);
     void kernel_times(double *ms5, long *counts5);
