@@ -1,8 +1,8 @@
 """The precision study (tests/precision_study.py) at a small size, with bounds: float32, float16 and
 bfloat16 storage against the FP64 oracle on noise with narrowband and zero-DM broadband RFI, rank 12
 from 4096 channels, the benchmark's 5-tree layout, one beam, four chunks. The bounds hold the
-measured errors with margin (at rank 16 the same study gives 6.6e-3 sigma and 1.3e-3 relative for
-float16)."""
+measured errors with margin (at rank 16, 8 beams x 64 chunks, the same study gives 7.2e-3 sigma and
+1.3e-3 relative for float16)."""
 
 import pytest
 
