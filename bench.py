@@ -406,6 +406,18 @@ def run_spill(steps, beams=8, clag=2):
     res = dict(value=round(beams * CHUNK_SECONDS / (ms * 1e-3), 2), unit="beams", ms_per_step=round(ms, 4), beams=beams,
                max_gpu_clag=clag, device_bytes=dd.device_bytes(), host_bytes=dd.host_bytes(),
                device_bytes_per_beam=round(dd.device_bytes() / beams / 1e9, 3))
+    # Beams whose state fits at this max_gpu_clag: the fewer of what the GPU's HBM and the host's
+    # memory hold (device and host bytes per beam).
+    try:
+        import psutil
+        host_total = psutil.virtual_memory().total
+        hbm = torch.cuda.get_device_properties(torch.cuda.current_device()).total_memory
+        per_dev, per_host = dd.device_bytes() / beams, dd.host_bytes() / beams
+        res["capacity_beams"] = int(min(hbm // per_dev, host_total // per_host if per_host else hbm // per_dev))
+        res["capacity_note"] = ("min(HBM %.0f GB / %.2f GB per beam, host memory %.0f GB / %.2f GB per beam)"
+                                % (hbm / 1e9, per_dev / 1e9, host_total / 1e9, per_host / 1e9))
+    except Exception:
+        pass
     del dd
     torch.cuda.empty_cache()
     return res
