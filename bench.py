@@ -702,6 +702,16 @@ def main():
         except Exception:
             traffic = None
     alg_total = sum(r["alg"])
+    # Stage 2 and peak finding judged together as pirate's fused CoalescedDdKernel2
+    # (src_lib/CoalescedDdKernel2.cu:128-135): the stage-1 delay lines read once plus the outputs, which
+    # equals the peak finder's algorithmic bytes (its subband-row reads are the same count of samples);
+    # the subband rows' HBM round trip between the two kernels counts as overhead here.
+    t_cdd2 = (kt["stage2"][0] + kt["pf"][0]) / nsteps
+    cdd2 = None
+    if t_cdd2 > 0:
+        a_cdd2 = r["alg"][classes.index("pf")] / (t_cdd2 * 1e-3) / 1e9
+        cdd2 = {"achieved": round(a_cdd2, 1), "peak": peak, "unit": "GB/s", "frac": round(a_cdd2 / peak, 4),
+                "ms_per_step": round(t_cdd2, 4), "algorithmic_bytes_per_step": r["alg"][classes.index("pf")]}
     e2e_alg_gbs = alg_total / (r["ms_per_step"] * 1e-3) / 1e9
 
     line = None
@@ -724,6 +734,7 @@ def main():
                 "time_loop": {"value": round(r["time_loop"], 2), "unit": "beams", "iterations": r["time_loop_iters"],
                               "note": "pirate's GpuDedisperser::time loop (pb2_dd_time) on one GPU: int4 input copied from "
                                       "pinned host memory every batch, median over iterations"},
+                "cdd2_model": cdd2,
                 "kernel_timing": {"ms_per_step": round(r["kms_per_step"], 4), "steps": nsteps,
                                   "note": "per-kernel-class CUDA events in a second timed region of the same K steps"},
                 "pipeline_alg_GBps": round(e2e_alg_gbs, 1),
