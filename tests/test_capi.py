@@ -173,6 +173,12 @@ def test_new_entry_points_validate_arguments(pb2lib):
     fails(L.pb2_pulse_inject(h, None, 0, 10, 256, 256, 0, 1.0, None), "null")
     fails(L.pb2_pulse_add_to_timestream(h, buf.ctypes.data, 9, 4, 4, 0, 1.0), "row per channel")
     L.pb2_pulse_destroy(h)
+    # the timing loop: null arguments, and a dedisperser that was never allocated (no device work)
+    rtb = np.zeros(8)
+    fails(L.pb2_dd_time(None, 8, rtb.ctypes.data_as(dp)), "null")
+    dd = pb2lib.GpuDedisperser(plan, cuda_device_id=0, num_consumers=1)
+    fails(L.pb2_dd_time(dd._h, 8, None), "null")
+    fails(L.pb2_dd_time(dd._h, 8, rtb.ctypes.data_as(dp)), "allocate")
 
 
 def test_kernel_launches_per_batch(pb2lib):
