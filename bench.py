@@ -369,7 +369,7 @@ def run_batched(scale, steps, reps=3):
     return res
 
 
-def run_spill(steps, beams=8, clag=2):
+def run_spill(steps, beams=8, clag=2, sweep=True):
     """The benchmark plan with delay lines more than 'clag' chunks deep in pinned host memory (g2h/h2g
     copy kernels every chunk): real-time beams, device and host bytes."""
     import torch
@@ -420,7 +420,33 @@ def run_spill(steps, beams=8, clag=2):
         pass
     del dd
     torch.cuda.empty_cache()
+    if sweep:
+        res["capacity_by_clag"] = spill_capacity()
     return res
+
+
+def spill_capacity(clags=(1, 2, 4, 8, 16, 32)):
+    """Beams whose state fits in HBM plus host memory, for several max_gpu_clag values: device and
+    host bytes of a one-beam dedisperser of the benchmark plan (an upper bound per beam, fixed buffers
+    included), the fewer of HBM / device bytes and host memory / host bytes."""
+    import torch
+    import psutil
+    import pirate_b200 as pb
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    hbm = torch.cuda.get_device_properties(dev).total_memory
+    host = psutil.virtual_memory().total
+    out = []
+    for clag in clags:
+        cfg = bench_config(1, "float16")
+        cfg["max_gpu_clag"] = clag
+        dd = pb.GpuDedisperser(pb.DedispersionPlan(pb.DedispersionConfig.from_dict(cfg)), cuda_device_id=dev, num_consumers=1)
+        dd.allocate()
+        d, h = dd.device_bytes(), dd.host_bytes()
+        del dd
+        torch.cuda.empty_cache()
+        out.append({"max_gpu_clag": clag, "device_gb_per_beam": round(d / 1e9, 3), "host_gb_per_beam": round(h / 1e9, 3),
+                    "beams": int(min(hbm // d, host // h if h else hbm // d))})
+    return out
 
 
 def run_sifter(steps, beams=8, n_train=6144, n_test=3072):
@@ -776,6 +802,10 @@ def main():
                                         "state (fp16), more than this GPU's HBM plus host memory" % args.batched_scale)
     if world == 1 and not args.no_spill:
         line["spill"] = run_spill(max(5, min(args.steps, 10)))
+        # the same at the max_gpu_clag that fits the most beams (the sweep above): fewer, deeper rows spilled
+        deep = run_spill(max(5, min(args.steps, 10)), clag=32, sweep=False)
+        line["spill"]["max_gpu_clag_32"] = {k: deep[k] for k in ("value", "ms_per_step", "device_bytes_per_beam", "capacity_beams")
+                                            if k in deep}
     if world == 1 and not args.no_sifter:
         line["sifter"] = run_sifter(max(5, min(args.steps, 20)))
     if rank == 0:
