@@ -15,7 +15,7 @@ Multi-GPU: the path shards by beam with no exchange step, so N GPUs run N indepe
 value = all ranks' beams over the max-over-ranks time.
 
 Also reported on one GPU: the plain fp32 path (one beam, float32 storage and input, no batching;
-BASELINE's config 2 shape) as 'plain_fp32', and the number of beams whose lag state fits in HBM as
+the benchmark plan with fp32 storage) as 'plain_fp32', and the number of beams whose lag state fits in HBM as
 'capacity_beams'.
 """
 
@@ -315,8 +315,8 @@ def run_ours(args, rank, world):
                 bytes_per_beam=per_beam)
 
 
-def cfg3_groups(scale):
-    """BASELINE config 3's mix: tree ranks 12, 14, 16 in proportions 1:1:2 (64 beams at scale 1),
+def uneven_groups(scale):
+    """The uneven workload: tree ranks 12, 14, 16 in proportions 1:1:2 (64 beams at scale 1),
     downsampling depths (primary trees) 3, 4, 5 spread over each rank's beams, 2048-sample chunks,
     float16 storage; channels = 2^rank / 4 (the benchmark's 16384 channels for rank 16)."""
     out = []
@@ -339,12 +339,12 @@ def group_config(rank, depth, beams, dtype="float16", max_gpu_clag=10000):
 
 
 def run_batched(scale, steps, reps=3):
-    """BASELINE config 3 (uneven beams, one replayed CUDA graph per chunk, autotuned schedule): returns
+    """The uneven workload (beams of ranks 12/14/16, one replayed CUDA graph per chunk, autotuned schedule): returns
     the real-time beams, ms per step and the record. Inputs are N(0,1) float16 noise resident in every
     group's input slot."""
     import torch
     import pirate_b200 as pb
-    groups = cfg3_groups(scale)
+    groups = uneven_groups(scale)
     plans = [pb.DedispersionPlan(pb.DedispersionConfig.from_dict(group_config(r, d, b))) for r, d, b in groups]
     bd = pb.BatchedDedisperser(plans, cuda_device_id=int(os.environ.get("LOCAL_RANK", "0")))
     bd.allocate()
@@ -497,7 +497,7 @@ def run_sifter(steps, beams=8, n_train=6144, n_test=3072):
 
 
 def run_plain_fp32(args, steps):
-    """The plain fp32 GPU path (BASELINE config 2's shape): one beam, float32 storage, float32 N(0,1)
+    """The plain fp32 GPU path (the benchmark plan's shape): one beam, float32 storage, float32 N(0,1)
     input resident in the input slot (no int4 input, no batching), same plan otherwise. Returns
     (real-time beams, ms per step)."""
     import torch
@@ -630,10 +630,10 @@ def main():
     ap.add_argument("--streams", type=int, default=1, help="compute streams (num_active_batches); beams split into that many batches")
     ap.add_argument("--no-plain-fp32", action="store_true")
     ap.add_argument("--no-streams-leg", action="store_true", help="skip the two-compute-stream leg")
-    ap.add_argument("--no-batched", action="store_true", help="skip the config-3 batched leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the uneven-workload batched leg")
     ap.add_argument("--no-spill", action="store_true", help="skip the host-spill leg")
     ap.add_argument("--no-sifter", action="store_true", help="skip the learned-sifter leg")
-    ap.add_argument("--batched-scale", type=float, default=0.5, help="config 3's beam counts x this")
+    ap.add_argument("--batched-scale", type=float, default=0.5, help="the uneven workload's 64 beams x this")
     ap.add_argument("--dtype", default="float16", choices=["float16", "bfloat16", "float32"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -797,8 +797,8 @@ def main():
                               "config": "1 beam, float32 storage, float32 input resident on the device, no batching"}
         line["vs_plain_fp32"] = round(value / pv, 3)
     if world == 1 and not args.no_batched:
-        line["batched_cfg3"] = run_batched(args.batched_scale, max(10, min(args.steps, 30)))
-        line["batched_cfg3"]["note"] = ("config 3's mix at %g x its 64 beams: the full 64 need about 300 GB of lag "
+        line["batched_uneven"] = run_batched(args.batched_scale, max(10, min(args.steps, 30)))
+        line["batched_uneven"]["note"] = ("the uneven workload at %g x its 64 beams: the full 64 need about 300 GB of lag "
                                         "state (fp16), more than this GPU's HBM plus host memory" % args.batched_scale)
     if world == 1 and not args.no_spill:
         line["spill"] = run_spill(max(5, min(args.steps, 10)))

@@ -1,6 +1,6 @@
 """Training and evaluation of the learned candidate sifter on pipeline candidates.
 
-    python -m pirate_b200.sifter_study [--config cfg2|small] [--train N] [--test N] [--out results.json]
+    python -m pirate_b200.sifter_study [--config rank16|small] [--train N] [--test N] [--out results.json]
 
 Events come from pirate_b200.sifter.CandidateGenerator (pulses from pirate's simpulse model, N(0,1)
 noise, RFI) run through the dedispersion pipeline; the training events and the held-out test events
@@ -21,13 +21,13 @@ from pirate_b200 import sifter as S
 
 
 def config(name):
-    """cfg2: the benchmark's rank-16 pipeline (16384 channels, 5 primary trees, 2048-sample chunks,
+    """rank16: the benchmark's rank-16 pipeline (16384 channels, 5 primary trees, 2048-sample chunks,
     float16 storage), 8 beams per batch. small: rank 12 from 2048 channels, 1024-sample chunks."""
     def prim(rank, n, wt_time):
         return [dict(num_early_triggers=0, max_width=32, dm_downsampling=0, time_downsampling=0,
                      wt_dm_downsampling=2 ** ((rank - (1 if i else 0)) // 2), wt_time_downsampling=wt_time)
                 for i in range(n)]
-    if name == "cfg2":
+    if name == "rank16":
         rank, nfreq, nt = 16, 16384, 2048
     else:
         rank, nfreq, nt = 12, 2048, 1024
@@ -83,7 +83,7 @@ def study(cfg, n_train, n_test, epochs=40, batch=256, lr=2e-3, nbank=64, seed=0,
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", default="cfg2", choices=["cfg2", "small"])
+    ap.add_argument("--config", default="rank16", choices=["rank16", "small"])
     ap.add_argument("--train", type=int, default=40000)
     ap.add_argument("--test", type=int, default=20000)
     ap.add_argument("--epochs", type=int, default=40)
