@@ -728,7 +728,7 @@ def main():
         except Exception:
             traffic = None
     alg_total = sum(r["alg"])
-    # Stage 2 and peak finding judged together as pirate's fused CoalescedDdKernel2
+    # Stage 2 and peak finding counted together as pirate's fused CoalescedDdKernel2
     # (src_lib/CoalescedDdKernel2.cu:128-135): the stage-1 delay lines read once plus the outputs, which
     # equals the peak finder's algorithmic bytes (its subband-row reads are the same count of samples);
     # the subband rows' HBM round trip between the two kernels counts as overhead here.

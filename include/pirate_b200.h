@@ -243,7 +243,7 @@ int pb2_dd_kernel_times(pb2_dedisperser *dd, double *ms5, long *counts5);
 void pb2_dd_destroy(pb2_dedisperser *dd);
 
 /* ---- Learned candidate sifter (no counterpart in pirate: a learned stage behind the threshold peak
- * finder, which stays the fallback and the judge of its recall) ----
+ * finder, which stays the fallback and the yardstick of its recall) ----
  *
  * Patch: 9 fine DMs (the peak's +-4) x 32 output times x 6 trailing boxcar widths (1..32) of the
  * dedispersed data around a candidate, each boxcar sum / sqrt(width), fp16, layout (dm, time, width).

@@ -31,7 +31,7 @@ public:
     bool operator!() const { return true; }
     std::size_t size() const { return 0; }
     template<typename K> Node operator[](const K &) const { return Node(); }
-    template<typename T> T as() const { throw std::runtime_error("yaml-cpp shim: YAML parsing is not available in this build"); }
+    template<typename T> T as() const { throw std::runtime_error("yaml-cpp shim: YAML parsing is not available in this shim"); }
     const std::string &Scalar() const { static std::string s; return s; }
     struct iterator {
         bool operator!=(const iterator &) const { return false; }
@@ -43,8 +43,8 @@ public:
     iterator end() const { return iterator(); }
 };
 
-inline Node Load(const std::string &) { throw std::runtime_error("yaml-cpp shim: YAML parsing is not available in this build"); }
-inline Node LoadFile(const std::string &) { throw std::runtime_error("yaml-cpp shim: YAML parsing is not available in this build"); }
+inline Node Load(const std::string &) { throw std::runtime_error("yaml-cpp shim: YAML parsing is not available in this shim"); }
+inline Node LoadFile(const std::string &) { throw std::runtime_error("yaml-cpp shim: YAML parsing is not available in this shim"); }
 
 class Emitter
 {

@@ -9,7 +9,7 @@
 // compressed as 8 asinh(x / 8) (linear within +-8 sigma, logarithmic beyond), stored fp16.
 // The sifter is an MLP 1728 -> 256 -> 128 -> 1 (ReLU) with bf16 weights and FP32 accumulation on the
 // tensor cores (mma.sync m16n8k16 bf16), trained with its own forward/backward/Adam kernels on the
-// binary cross-entropy of the logit. The threshold peak finder stays the fallback and the judge of the
+// binary cross-entropy of the logit. The threshold peak finder stays the fallback and the yardstick of the
 // sifter's recall and false-alarm rate.
 
 #pragma once

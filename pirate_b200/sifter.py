@@ -1,5 +1,5 @@
 """The learned candidate sifter behind the threshold peak finder (no pirate counterpart; the plain
-threshold stays the fallback and the judge of the sifter's recall and false-alarm rate).
+threshold stays the fallback and the yardstick of the sifter's recall and false-alarm rate).
 
 - ``Sifter``: the MLP 1728 -> 256 -> 128 -> 1 (bf16 weights, FP32 accumulation) with its CUDA forward,
   backward and Adam kernels (``libpirate_b200.so``: ``pb2_sifter_*``).
